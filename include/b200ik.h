@@ -1,0 +1,274 @@
+/*
+ * b200ik.h — C ABI of libb200ik.so, the sm_100a batched Levenberg–Marquardt
+ * inverse-kinematics library.
+ *
+ * Every entry point returns an int status: 0 on success, a negative IK_E_*
+ * code on an API error (the message is kept per host thread and returned by
+ * ik_last_error()).  Per-problem numerical outcomes (converged, iteration cap,
+ * non-SPD normal matrix, non-finite input) are written to an int32 status array
+ * on the device instead.  No C++ exception crosses this boundary.
+ *
+ * Pointers named d_* are device pointers owned by the caller; the library
+ * never retains them beyond the call, except the pose-target pointers a term
+ * descriptor names, which are read at every solve (like the target arrays a
+ * reference term keeps, robokit terms/dense/position_task.py:77).  All calls are
+ * stream-ordered on the caller's stream (a cudaStream_t passed as void*, 0 for
+ * the legacy default stream) and do not synchronise the device.
+ *
+ * Pose layout everywhere: 7 floats [x, y, z, qw, qx, qy, qz], the reference's
+ * vec7 (robokit AGENTS.md "SE(3)"; xform/warp/rotation_conversions.py:268).
+ * Tangent layout of one problem: [6 floating-base twist entries, if floating |
+ * one entry per actuated joint] (robo/robot_state.py:178-181).
+ */
+#ifndef B200IK_H
+#define B200IK_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define IK_OK 0
+#define IK_E_INVALID (-1)     /* bad argument / inconsistent tables           */
+#define IK_E_CAPACITY (-2)    /* batch larger than the problem's capacity     */
+#define IK_E_OOM (-3)         /* device allocation failed                     */
+#define IK_E_CUDA (-4)        /* a CUDA runtime call failed                   */
+#define IK_E_UNSUPPORTED (-5) /* a size beyond the kernel's compiled limits   */
+#define IK_E_NO_DEVICE (-6)   /* no CUDA device visible                       */
+
+/* per-problem status bits written by the solvers */
+#define IK_ST_RUNNING 0
+#define IK_ST_CONVERGED 1   /* a per-problem stop rule fired                  */
+#define IK_ST_MAX_ITER 2    /* iteration cap reached                          */
+#define IK_ST_NOT_SPD 4     /* some damped normal matrix had a pivot <= 0     */
+#define IK_ST_NONFINITE 8   /* non-finite cost at the start point             */
+
+/* joint types, robo/robot_spec.py:34-41 */
+#define IK_JOINT_FIXED 0
+#define IK_JOINT_PRISMATIC 1
+#define IK_JOINT_REVOLUTE 2
+
+/* term kinds */
+#define IK_TERM_POSITION 1       /* terms/dense/position_task.py:18            */
+#define IK_TERM_ROTATION 2       /* terms/dense/rotation_task.py:25            */
+#define IK_TERM_POSITION_LIMIT 3 /* terms/dense/position_limit.py:185 ("abs")  */
+#define IK_TERM_SELF_COLLISION 4 /* terms/dense/self_collision_task.py:593     */
+
+/* self-collision pair modes */
+#define IK_PAIRS_SLOTS 0 /* reference: <= K link pairs, most penetrating sphere pair each */
+#define IK_PAIRS_ALL 1   /* every filtered sphere pair is one residual row              */
+
+/* stop rules (bitmask) */
+#define IK_STOP_NONE 0
+#define IK_STOP_ALL_COST 1 /* reference rule: stop once every problem's cost <= cost_tol (opt/optimizer.py:237-239) */
+#define IK_STOP_STEP 2     /* per problem: ||delta||_2 < step_tol                                             */
+#define IK_STOP_POSE 4     /* per problem: every pose target within pose_pos_tol [m] and pose_rot_tol [rad]   */
+#define IK_STOP_COST 8     /* per problem: cost <= cost_tol                                                   */
+
+/* ---- robot model ------------------------------------------------------- */
+/* The kinematic tables of robo/robot_spec.py:65-139 (RobotSpec) after
+ * parsing; arrays are host pointers copied at ik_robot_create. */
+typedef struct IkRobotDesc {
+    int32_t num_joints;   /* all joints, fixed included (<= 64)                 */
+    int32_t num_links;    /* (<= 128)                                           */
+    int32_t num_actuated; /* (<= 64 together with a floating base's 6)          */
+    int32_t num_spheres;  /* collision spheres, 0 if none (<= 256)              */
+    const int32_t* joint_types;       /* [nj]                                     */
+    const float* joint_axes;          /* [nj*3]                                   */
+    const float* parent_transforms;   /* [nj*7] joint origin in its parent joint  */
+    const int32_t* parent_joints;     /* [nj] -1 = attached to the base link      */
+    const int32_t* actuated_indices;  /* [nj] -1 = not actuated                   */
+    const int32_t* mimic_indices;     /* [nj] actuated index mimicked, -1 = none  */
+    const float* mimic_multipliers;   /* [nj]                                     */
+    const float* mimic_offsets;       /* [nj]                                     */
+    const int32_t* link_parent_joints;/* [nl] -1 = base link                      */
+    const float* actuated_limits;     /* [na*2] lower, upper                      */
+    const float* sphere_centers;      /* [ns*3] link-local                        */
+    const float* sphere_radii;        /* [ns]                                     */
+    const int32_t* sphere_links;      /* [ns]                                     */
+    const float* link_bound_centers;  /* [nl*3] link-local bounding-sphere centre */
+    const float* link_bound_radii;    /* [nl]                                     */
+} IkRobotDesc;
+
+typedef struct IkRobot IkRobot;
+typedef struct IkProblem IkProblem;
+
+/* ---- cost terms -------------------------------------------------------- */
+typedef struct IkTermDesc {
+    int32_t kind;                 /* IK_TERM_*                                         */
+    /* pose terms */
+    int32_t num_frames;
+    const int32_t* frame_links;   /* [num_frames] link indices                         */
+    const float* weights;         /* position/rotation: [num_frames*3]; limit: [na];
+                                     self-collision: [1]                                 */
+    const float* d_targets;       /* device [capacity rows, num_frames, 7] pose targets  */
+    int32_t target_rows;          /* rows of d_targets; problem b reads row
+                                     b / max(1, batch / target_rows) (reference n_repeat,
+                                     position_task.py:201-202)                           */
+    /* self-collision */
+    float margin;
+    int32_t max_active_pairs;     /* K, slots mode                                      */
+    int32_t pair_mode;            /* IK_PAIRS_*                                         */
+    int32_t num_link_pairs;
+    const int32_t* link_pairs;        /* [num_link_pairs*2] (link a, link b)            */
+    const int32_t* link_pair_offsets; /* [num_link_pairs+1] CSR into sphere_pairs        */
+    int32_t num_sphere_pairs;
+    const int32_t* sphere_pairs;      /* [num_sphere_pairs*2] grouped by link pair       */
+} IkTermDesc;
+
+/* LMOptimizerConfig (opt/lm_optimizer.py:503-523) + OptimizerConfig
+ * (opt/optimizer.py:160-167) + the per-problem stop rules. */
+typedef struct IkLmParams {
+    int32_t max_iter;
+    float lambda_init;        /* lm_lambda                                   */
+    float lambda_factor;
+    float lambda_min;
+    float lambda_max;
+    float rho_min;
+    float gain_ratio_epsilon;
+    int32_t stop_rules;       /* IK_STOP_* bitmask                           */
+    float cost_tol;
+    float step_tol;
+    float pose_pos_tol;
+    float pose_rot_tol;
+    int32_t check_interval;   /* early_stopping_interval of IK_STOP_ALL_COST (>= 1) */
+} IkLmParams;
+
+/* ---- lifecycle ----------------------------------------------------------- */
+const char* ik_last_error(void);
+int ik_version(void);
+int ik_device_count(int* out);
+int ik_set_device(int device);
+
+int ik_robot_create(const IkRobotDesc* desc, IkRobot** out);
+int ik_robot_destroy(IkRobot* robot);
+
+/* A problem = robot + term list + tangent layout, with device buffers sized
+ * for `capacity` problems (opt/optimizer.py:313-333: buffers are sized at the
+ * first solve and smaller batches use a prefix).  `active_dof_mask` is a host
+ * float array [tangent_dim] or NULL (opt/optimizer.py:203). */
+int ik_problem_create(IkRobot* robot, int32_t capacity, int32_t floating_base, const IkTermDesc* terms,
+                      int32_t num_terms, const float* active_dof_mask, IkProblem** out);
+int ik_problem_destroy(IkProblem* problem);
+int ik_problem_info(const IkProblem* problem, int32_t* tangent_dim, int32_t* residual_dim, int32_t* capacity);
+/* Re-point a pose term's targets (set_target / resolve in the reference). */
+int ik_problem_set_targets(IkProblem* problem, int32_t term_index, const float* d_targets, int32_t target_rows);
+
+/* ---- solvers -------------------------------------------------------------- */
+/* Whole LM solve, the plain form: one kernel launch per iteration over the
+ * fixed batch, LMOptimizer.solve (opt/optimizer.py:216-240,
+ * opt/lm_optimizer.py:834-1005).  d_q [batch*na] and d_base [batch*7] (NULL
+ * without a floating base) are read as the start point and overwritten with
+ * the solution.  Outputs: d_cost [batch] final cost 0.5*|r|^2, d_lambda [batch]
+ * final damping, d_iters [batch] iterations run, d_status [batch] IK_ST_* bits.
+ * Any output may be NULL. */
+int ik_solve_plain(IkProblem* problem, int32_t batch, float* d_q, float* d_base, const IkLmParams* params,
+                   float* d_cost, float* d_lambda, int32_t* d_iters, int32_t* d_status, void* stream);
+
+/* The same solve with the LM loop of each problem inside one persistent
+ * launch: groups of lanes pull problems from a device work queue and iterate
+ * each to its stop rule (IK_STOP_ALL_COST is not available here). */
+int ik_solve_persistent(IkProblem* problem, int32_t batch, float* d_q, float* d_base, const IkLmParams* params,
+                        float* d_cost, float* d_lambda, int32_t* d_iters, int32_t* d_status, void* stream);
+
+/* Pick the lane-group width (8, 16 or 32 lanes per problem; 0 = automatic)
+ * and the resident groups per SM of the persistent form (0 = automatic). */
+int ik_problem_set_schedule(IkProblem* problem, int32_t group_lanes, int32_t blocks_per_sm);
+int ik_problem_get_schedule(const IkProblem* problem, int32_t* group_lanes, int32_t* blocks_per_sm);
+
+/* ---- single-stage kernels (parity and the per-term reference API) ---------- */
+/* Forward kinematics, Robot.forward_kinematics (robo/robot.py:131) with the
+ * motion subspace (robo/robot_kernels.py:651-664) and the collision spheres
+ * (robo/robot.py:428).  Outputs may be NULL: T_joint [B,nj,7], T_link [B,nl,7],
+ * S_world [B,6,nj], spheres [B,ns,3], link_bounds [B,nl,3]. */
+int ik_fk(IkRobot* robot, int32_t batch, const float* d_q, const float* d_base, float* d_T_joint, float* d_T_link,
+          float* d_S_world, float* d_spheres, float* d_link_bounds, void* stream);
+
+/* Link Jacobian, RobotState.get_link_jacobian (robo/robot_state.py:192,
+ * robo/robot_kernels.py:668-737): out [B,6,tangent], frame 0 spatial, 1 body. */
+int ik_link_jacobian(IkRobot* robot, int32_t batch, const float* d_q, const float* d_base, int32_t link,
+                     int32_t body_frame, float* d_J, void* stream);
+
+/* Weighted residuals and Jacobians of every term in the reference's row
+ * layout (terms in order, LMOptimizer._default_offsets, lm_optimizer.py:594-602):
+ * d_r [B,R], d_J [B,R,tangent] (either may be NULL). */
+int ik_residual_jacobian(IkProblem* problem, int32_t batch, const float* d_q, const float* d_base, float* d_r,
+                         float* d_J, void* stream);
+
+/* Normal equations as the fused kernel forms them (lm_optimizer.py:145-189):
+ * d_H [B,D,D], d_g [B,D], d_cost [B]. */
+int ik_normal_equations(IkProblem* problem, int32_t batch, const float* d_q, const float* d_base, float* d_H,
+                        float* d_g, float* d_cost, void* stream);
+
+/* Damped FP64 Cholesky step (lm_optimizer.py:56-79): delta = -(H + lambda I)^-1 g,
+ * pred = 0.5 * delta . (lambda delta - g).  d_H [B,D,D], d_g [B,D], d_lambda [B]
+ * in; d_delta [B,D], d_pred [B] out; d_spd [B] (may be NULL) 1 if factorable. */
+int ik_damped_solve(int32_t batch, int32_t dim, const float* d_H, const float* d_g, const float* d_lambda,
+                    float* d_delta, float* d_pred, int32_t* d_spd, void* stream);
+
+/* One LM iteration with the reference's buffers (LMOptimizer._step_body):
+ * in/out d_q, d_base, d_lambda; out d_cost (the `costs` buffer after the step:
+ * the proposal's cost if accepted, else the start point's), d_delta [B,D],
+ * d_pred [B], d_cost_new [B] (the proposal's cost), d_accept [B]. */
+int ik_step(IkProblem* problem, int32_t batch, float* d_q, float* d_base, float* d_lambda, const IkLmParams* params,
+            float* d_cost, float* d_delta, float* d_pred, float* d_cost_new, int32_t* d_accept, void* stream);
+
+/* Gain-ratio accept/reject and lambda update on scalars
+ * (lm_accept_reject_cost_kernel, lm_optimizer.py:338-362), FP64 ratio. */
+int ik_accept_reject(int32_t batch, float* d_cost, const float* d_cost_new, const float* d_pred, float* d_lambda,
+                     int32_t* d_accept, const IkLmParams* params, void* stream);
+
+/* IK accuracy metrics (helpers/ik/ik.py:60-82): per target position error [m]
+ * and angle error [rad], success when every target is under both thresholds. */
+int ik_metrics(IkRobot* robot, int32_t batch, const float* d_q, const float* d_base, int32_t num_targets,
+               const int32_t* d_target_links, const float* d_targets, float pos_threshold, float rot_threshold,
+               float* d_pos_err, float* d_rot_err, int32_t* d_success, void* stream);
+
+/* Integrate a tangent step, RobotState.integrate (robo/robot_state.py:238-312):
+ * q' = q + mask*delta, base' = base * exp(delta_base) (eps 1e-4). */
+int ik_integrate(int32_t batch, int32_t num_actuated, int32_t floating_base, const float* d_q, const float* d_base,
+                 const float* d_delta, const float* d_mask, float* d_q_out, float* d_base_out, void* stream);
+
+/* Strided row copy: dst[r*dst_stride + c] = src[r*src_stride + c], c < width
+ * (the row_offset writes of compute_weighted_residual, task.py:150-167, and
+ * RobotState.get_T_world_link, robo/robot_state.py:186-190). */
+int ik_copy_rows(int32_t rows, int32_t width, const float* d_src, int64_t src_stride, float* d_dst, int64_t dst_stride,
+                 void* stream);
+
+/* Masked row copy, RobotState.accept (robo/robot_state.py:448-476,
+ * robot_kernels.py:744-767): rows with d_mask[r] == 1 copy `width` floats. */
+int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, const float* d_src, float* d_dst,
+                        void* stream);
+
+/* Clamp joints to [lo, hi], RobotState.clamp_q (robo/robot_state.py:314-333,
+ * robot_kernels.py:593-609); entries whose d_mask is 0 are left (mask may be NULL). */
+int ik_clamp_q(int32_t batch, int32_t num_actuated, float* d_q, const float* d_limits, const float* d_mask,
+               void* stream);
+
+/* ---- device memory, streams, events (the package imports no torch) ------ */
+int ik_malloc(void** d_ptr, size_t bytes);
+int ik_free(void* d_ptr);
+int ik_malloc_host(void** h_ptr, size_t bytes); /* pinned */
+int ik_free_host(void* h_ptr);
+int ik_memcpy_htod(void* d_dst, const void* h_src, size_t bytes, void* stream);
+int ik_memcpy_dtoh(void* h_dst, const void* d_src, size_t bytes, void* stream);
+int ik_memcpy_dtod(void* d_dst, const void* d_src, size_t bytes, void* stream);
+int ik_memset(void* d_ptr, int value, size_t bytes, void* stream);
+int ik_stream_create(void** stream);
+int ik_stream_destroy(void* stream);
+int ik_stream_synchronize(void* stream);
+int ik_device_synchronize(void);
+int ik_event_create(void** event);
+int ik_event_destroy(void* event);
+int ik_event_record(void* event, void* stream);
+int ik_event_elapsed_ms(void* start, void* stop, float* ms);
+/* Count of this library's kernel launches since load (for launch accounting). */
+int ik_launch_count(int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200IK_H */

@@ -1,0 +1,1186 @@
+// ik_api.cu — host side of libb200ik.so: validation, table lowering, launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "b200ik.h"
+#include "ik_kernels.cuh"
+
+using namespace b200ik;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) return fail(IK_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ----------------------------------------------------------------------------
+// host copy of a robot
+// ----------------------------------------------------------------------------
+struct RobotHost {
+    int nj = 0, nl = 0, na = 0, ns = 0;
+    std::vector<int> jtype, jparent, jact, jmimic, lpj, sphlink;
+    std::vector<float> jmul, joff, jaxis, jpt, lim, sph, lbound;
+    std::vector<unsigned long long> lanc;  // per link: ancestor joints
+    std::vector<int> colstart, coljoint;
+    std::vector<float> colmul;
+    int fk_rounds = 0;
+};
+
+struct BlobBuilder {
+    std::vector<char> buf;
+    BlobBuilder() { buf.resize((sizeof(TabHeader) + 15) & ~size_t(15), 0); }
+    int add(const void* p, size_t bytes) {
+        const size_t off = buf.size();
+        const size_t padded = (bytes + 15) & ~size_t(15);
+        buf.resize(off + (padded ? padded : 16), 0);
+        if (bytes) std::memcpy(buf.data() + off, p, bytes);
+        return (int)off;
+    }
+    template <typename T>
+    int addv(const std::vector<T>& v) { return add(v.data(), v.size() * sizeof(T)); }
+    TabHeader* hdr() { return reinterpret_cast<TabHeader*>(buf.data()); }
+};
+
+struct TermHost {
+    IkTermDesc d;
+    std::vector<int> frame_links;
+    std::vector<float> weights;
+    std::vector<int> lp, lpoff, sp;
+    int row = 0, rows = 0;
+};
+
+}  // namespace
+
+struct IkRobot {
+    RobotHost h;
+    char* d_blob[2] = {nullptr, nullptr};  // robot-only blobs: fixed base / floating base
+    int blob_bytes[2] = {0, 0};
+    int ws_bytes[2] = {0, 0};
+};
+
+struct IkProblem {
+    IkRobot* robot = nullptr;
+    int capacity = 0, floating = 0, D = 0, R = 0, E = 0;
+    std::vector<TermHost> terms;
+    std::vector<float> mask;
+    int mask_any = 0;
+    std::vector<char> blob;
+    char* d_blob = nullptr;
+    int blob_bytes = 0, ws_bytes = 0;
+    float* d_rec = nullptr;
+    int* d_counters = nullptr;
+    int* d_queue = nullptr;
+    int group = 0;          // 0 = automatic
+    int blocks_per_sm = 0;  // 0 = automatic
+};
+
+namespace {
+
+int num_sms() {
+    static int sms = -1;
+    if (sms < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+int max_smem_optin() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (v <= 0) v = 227 * 1024;
+    }
+    return v;
+}
+
+inline int al16(int x) { return (x + 15) & ~15; }
+
+// Workspace layout of one group.  Returns bytes.
+int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_sph, bool need_lbw) {
+    int off = 0;
+    auto take = [&](int bytes) {
+        const int o = off;
+        off += al16(std::max(bytes, 16));
+        return o;
+    };
+    const int nj = h->nj, nl = h->nl, na = h->na, ns = h->ns, D = h->D;
+    h->w_T0 = take(nj * 8 * 4);
+    h->w_T1 = take(nj * 8 * 4);
+    h->w_anc = take(2 * nj * 4);
+    h->w_sph = take(need_sph ? ns * 16 : 0);
+    h->w_lbw = take(need_lbw ? nl * 16 : 0);
+    h->w_tgt = take(npose * 8 * 4);
+    h->w_rpose = take(npose * 3 * 4);
+    h->w_rlim = take(na * 4);
+    h->w_Jc = take(kChunkRows * h->Dp * 4);
+    h->w_rc = take(kChunkRows * 4);
+    h->w_rowmeta = take(kChunkRows * 8 * 4);
+    h->w_Hs = take(h->E * 4);
+    h->w_Hc = take(h->E * 4);
+    h->w_L = take(h->T * 8);
+    h->w_tmp = take(D * 8);
+    h->w_y = take(D * 8);
+    h->w_q = take(na * 4);
+    h->w_qp = take(na * 4);
+    h->w_base = take(32);
+    h->w_basep = take(32);
+    h->w_d32 = take(D * 4);
+    h->w_misc = take(64 * 4);
+    const int slots_off = take(ncoll_slots_bytes);
+    h->ws_bytes = off;
+    return slots_off;
+}
+
+void add_robot_tables(BlobBuilder& b, const RobotHost& r) {
+    TabHeader* h = b.hdr();
+    h->nj = r.nj;
+    h->nl = r.nl;
+    h->na = r.na;
+    h->ns = r.ns;
+    h->fk_rounds = r.fk_rounds;
+    int o;
+    o = b.addv(r.jtype); b.hdr()->o_jtype = o;
+    o = b.addv(r.jparent); b.hdr()->o_jparent = o;
+    o = b.addv(r.jact); b.hdr()->o_jact = o;
+    o = b.addv(r.jmimic); b.hdr()->o_jmimic = o;
+    o = b.addv(r.jmul); b.hdr()->o_jmul = o;
+    o = b.addv(r.joff); b.hdr()->o_joff = o;
+    o = b.addv(r.jaxis); b.hdr()->o_jaxis = o;
+    o = b.addv(r.jpt); b.hdr()->o_jpt = o;
+    o = b.addv(r.lpj); b.hdr()->o_lpj = o;
+    o = b.addv(r.lanc); b.hdr()->o_lanc = o;
+    o = b.addv(r.lbound); b.hdr()->o_lbound = o;
+    o = b.addv(r.sph); b.hdr()->o_sph = o;
+    o = b.addv(r.sphlink); b.hdr()->o_sphlink = o;
+    o = b.addv(r.lim); b.hdr()->o_lim = o;
+    o = b.addv(r.colstart); b.hdr()->o_colstart = o;
+    o = b.addv(r.coljoint); b.hdr()->o_coljoint = o;
+    o = b.addv(r.colmul); b.hdr()->o_colmul = o;
+}
+
+std::vector<uint16_t> ab_table(int D) {
+    std::vector<uint16_t> ab;
+    for (int a = 0; a < D; ++a)
+        for (int c = 0; c <= a; ++c) ab.push_back((uint16_t)((a << 8) | c));
+    return ab;
+}
+
+// A blob with robot tables, no terms; used by FK / Jacobian / metrics kernels.
+void build_robot_blob(const RobotHost& r, int floating, std::vector<char>& out, int& ws_bytes) {
+    BlobBuilder b;
+    add_robot_tables(b, r);
+    TabHeader* h = b.hdr();
+    h->D = (floating ? 6 : 0) + r.na;
+    h->base_off = floating ? 6 : 0;
+    h->T = h->D * (h->D + 1) / 2;
+    h->E = h->T + h->D;
+    h->Dp = h->D;
+    std::vector<float> mask(h->D, 1.f);
+    int o = b.addv(mask);
+    b.hdr()->o_mask = o;
+    std::vector<uint16_t> ab = ab_table(b.hdr()->D);
+    o = b.addv(ab);
+    b.hdr()->o_ab = o;
+    h = b.hdr();
+    h->o_pose = h->o_coll = h->o_limw = h->o_mask;
+    layout_workspace(h, 0, 0, r.ns > 0, r.nl > 0);
+    h->bytes = (int)b.buf.size();
+    ws_bytes = h->ws_bytes;
+    out = b.buf;
+}
+
+int smem_bytes(int blob_bytes, int ws_bytes, int G) { return blob_bytes + (kBlockThreads / G) * ws_bytes; }
+
+int choose_group(int D, int blob_bytes, int ws_bytes, int requested) {
+    if (requested) return requested;
+    int G = D <= 8 ? 8 : (D <= 16 ? 16 : 32);
+    while (G < 32 && smem_bytes(blob_bytes, ws_bytes, G) > max_smem_optin()) G *= 2;
+    return G;
+}
+
+template <typename K>
+int prepare_kernel(K kernel, int smem) {
+    if (smem > max_smem_optin()) return fail(IK_E_UNSUPPORTED, "shared memory %d B exceeds the device limit", smem);
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return IK_OK;
+}
+
+template <typename K>
+int grid_for(K kernel, int smem, int batch, int G, int blocks_per_sm_req, int& grid) {
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlockThreads, smem));
+    if (per_sm <= 0) return fail(IK_E_UNSUPPORTED, "kernel does not fit on an SM (smem %d B)", smem);
+    if (blocks_per_sm_req > 0) per_sm = std::min(per_sm, blocks_per_sm_req);
+    const int gpb = kBlockThreads / G;
+    const int need = (batch + gpb - 1) / gpb;
+    grid = std::max(1, std::min(need, per_sm * num_sms()));
+    return IK_OK;
+}
+
+int check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(IK_E_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+    g_launches.fetch_add(1);
+    return IK_OK;
+}
+
+// Dispatch a templated kernel on the group width.
+#define IK_DISPATCH(G, KERNEL, ...)                                   \
+    do {                                                              \
+        switch (G) {                                                  \
+            case 8: { auto kfn = KERNEL<8>; __VA_ARGS__; break; }     \
+            case 16: { auto kfn = KERNEL<16>; __VA_ARGS__; break; }   \
+            case 32: { auto kfn = KERNEL<32>; __VA_ARGS__; break; }   \
+            default: return fail(IK_E_INVALID, "group width %d not in {8,16,32}", G); \
+        }                                                             \
+    } while (0)
+
+int validate_robot(const IkRobotDesc* d) {
+    if (!d) return fail(IK_E_INVALID, "robot descriptor is NULL");
+    if (d->num_joints < 0 || d->num_joints > kMaxJoints)
+        return fail(IK_E_UNSUPPORTED, "num_joints %d outside [0, %d]", d->num_joints, kMaxJoints);
+    if (d->num_links < 1 || d->num_links > kMaxLinks)
+        return fail(IK_E_UNSUPPORTED, "num_links %d outside [1, %d]", d->num_links, kMaxLinks);
+    if (d->num_actuated < 0 || d->num_actuated + 6 > kMaxDim + 6 || d->num_actuated > kMaxDim)
+        return fail(IK_E_UNSUPPORTED, "num_actuated %d outside [0, %d]", d->num_actuated, kMaxDim);
+    if (d->num_spheres < 0 || d->num_spheres > kMaxSpheres)
+        return fail(IK_E_UNSUPPORTED, "num_spheres %d outside [0, %d]", d->num_spheres, kMaxSpheres);
+    const int nj = d->num_joints, nl = d->num_links, na = d->num_actuated, ns = d->num_spheres;
+    if (nj > 0 && (!d->joint_types || !d->joint_axes || !d->parent_transforms || !d->parent_joints ||
+                   !d->actuated_indices || !d->mimic_indices || !d->mimic_multipliers || !d->mimic_offsets))
+        return fail(IK_E_INVALID, "joint tables must be non-NULL");
+    if (!d->link_parent_joints) return fail(IK_E_INVALID, "link_parent_joints is NULL");
+    if (na > 0 && !d->actuated_limits) return fail(IK_E_INVALID, "actuated_limits is NULL");
+    if (ns > 0 && (!d->sphere_centers || !d->sphere_radii || !d->sphere_links))
+        return fail(IK_E_INVALID, "sphere tables must be non-NULL");
+    for (int j = 0; j < nj; ++j) {
+        const int ty = d->joint_types[j];
+        if (ty < 0 || ty > 2) return fail(IK_E_INVALID, "joint %d has type %d", j, ty);
+        const int p = d->parent_joints[j];
+        if (p < -1 || p >= nj) return fail(IK_E_INVALID, "joint %d parent %d out of range", j, p);
+        const int a = d->actuated_indices[j], m = d->mimic_indices[j];
+        if (a < -1 || a >= na) return fail(IK_E_INVALID, "joint %d actuated index %d out of range", j, a);
+        if (m < -1 || m >= na) return fail(IK_E_INVALID, "joint %d mimic index %d out of range", j, m);
+        for (int k = 0; k < 7; ++k)
+            if (!std::isfinite(d->parent_transforms[7 * j + k]))
+                return fail(IK_E_INVALID, "joint %d parent transform is not finite", j);
+        if (ty != 0) {
+            const float* ax = d->joint_axes + 3 * j;
+            const float n = std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+            if (!(n > 0.f) || !std::isfinite(n)) return fail(IK_E_INVALID, "joint %d has a zero-length axis", j);
+        }
+    }
+    // the parent relation must be a forest: walking up from every joint ends
+    for (int j = 0; j < nj; ++j) {
+        int cur = j, steps = 0;
+        while (cur != -1) {
+            cur = d->parent_joints[cur];
+            if (++steps > nj) return fail(IK_E_INVALID, "joint parent table has a cycle through joint %d", j);
+        }
+    }
+    for (int l = 0; l < nl; ++l) {
+        const int pj = d->link_parent_joints[l];
+        if (pj < -1 || pj >= nj) return fail(IK_E_INVALID, "link %d parent joint %d out of range", l, pj);
+    }
+    for (int s = 0; s < ns; ++s) {
+        const int l = d->sphere_links[s];
+        if (l < 0 || l >= nl) return fail(IK_E_INVALID, "sphere %d link %d out of range", s, l);
+    }
+    return IK_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+const char* ik_last_error(void) { return g_last_error.c_str(); }
+int ik_version(void) { return 10000; }
+
+int ik_device_count(int* out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *out = 0;
+        return fail(IK_E_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    *out = n;
+    return IK_OK;
+}
+
+int ik_set_device(int device) {
+    CK(cudaSetDevice(device));
+    return IK_OK;
+}
+
+int ik_launch_count(int64_t* out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    *out = g_launches.load();
+    return IK_OK;
+}
+
+int ik_robot_create(const IkRobotDesc* d, IkRobot** out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = validate_robot(d);
+    if (rc) return rc;
+    IkRobot* R = new IkRobot();
+    RobotHost& r = R->h;
+    r.nj = d->num_joints;
+    r.nl = d->num_links;
+    r.na = d->num_actuated;
+    r.ns = d->num_spheres;
+    const int nj = r.nj, nl = r.nl, na = r.na, ns = r.ns;
+    r.jtype.assign(d->joint_types, d->joint_types + nj);
+    r.jparent.assign(d->parent_joints, d->parent_joints + nj);
+    r.jact.assign(d->actuated_indices, d->actuated_indices + nj);
+    r.jmimic.assign(d->mimic_indices, d->mimic_indices + nj);
+    r.jmul.assign(d->mimic_multipliers, d->mimic_multipliers + nj);
+    r.joff.assign(d->mimic_offsets, d->mimic_offsets + nj);
+    r.jaxis.assign(4 * nj, 0.f);
+    r.jpt.assign(8 * nj, 0.f);
+    for (int j = 0; j < nj; ++j) {
+        for (int k = 0; k < 3; ++k) r.jaxis[4 * j + k] = d->joint_axes[3 * j + k];
+        for (int k = 0; k < 7; ++k) r.jpt[8 * j + k] = d->parent_transforms[7 * j + k];
+    }
+    r.lpj.assign(d->link_parent_joints, d->link_parent_joints + nl);
+    r.lim.assign(2 * na, 0.f);
+    for (int i = 0; i < 2 * na; ++i) r.lim[i] = d->actuated_limits[i];
+    r.sph.assign(4 * std::max(ns, 0), 0.f);
+    r.sphlink.assign(ns, 0);
+    for (int s = 0; s < ns; ++s) {
+        for (int k = 0; k < 3; ++k) r.sph[4 * s + k] = d->sphere_centers[3 * s + k];
+        r.sph[4 * s + 3] = d->sphere_radii[s];
+        r.sphlink[s] = d->sphere_links[s];
+    }
+    r.lbound.assign(4 * nl, 0.f);
+    if (d->link_bound_centers && d->link_bound_radii)
+        for (int l = 0; l < nl; ++l) {
+            for (int k = 0; k < 3; ++k) r.lbound[4 * l + k] = d->link_bound_centers[3 * l + k];
+            r.lbound[4 * l + 3] = d->link_bound_radii[l];
+        }
+    // ancestors of each link (robot_spec.py:1133-1142)
+    r.lanc.assign(nl, 0ull);
+    for (int l = 0; l < nl; ++l) {
+        int j = r.lpj[l];
+        while (j != -1) {
+            r.lanc[l] |= 1ull << j;
+            j = r.jparent[j];
+        }
+    }
+    // tangent column -> contributing joints (robot_spec.py:1119-1131)
+    r.colstart.assign(na + 1, 0);
+    for (int a = 0; a < na; ++a) {
+        r.colstart[a] = (int)r.coljoint.size();
+        for (int j = 0; j < nj; ++j) {
+            if (r.jact[j] == a) {
+                r.coljoint.push_back(j);
+                r.colmul.push_back(1.f);
+            } else if (r.jact[j] < 0 && r.jmimic[j] == a) {
+                r.coljoint.push_back(j);
+                r.colmul.push_back(r.jmul[j]);
+            }
+        }
+    }
+    r.colstart[na] = (int)r.coljoint.size();
+    if (r.coljoint.empty()) {
+        r.coljoint.push_back(0);
+        r.colmul.push_back(0.f);
+    }
+    // pointer-jumping rounds
+    int maxd = 0;
+    for (int j = 0; j < nj; ++j) {
+        int dpt = 0, cur = j;
+        while (cur != -1) {
+            ++dpt;
+            cur = r.jparent[cur];
+        }
+        maxd = std::max(maxd, dpt);
+    }
+    int rounds = 0;
+    while ((1 << rounds) < maxd) ++rounds;
+    r.fk_rounds = rounds;
+    for (int f = 0; f < 2; ++f) {
+        std::vector<char> blob;
+        int ws = 0;
+        build_robot_blob(r, f, blob, ws);
+        R->blob_bytes[f] = (int)blob.size();
+        R->ws_bytes[f] = ws;
+        cudaError_t e = cudaMalloc(&R->d_blob[f], blob.size());
+        if (e != cudaSuccess) {
+            ik_robot_destroy(R);
+            return fail(IK_E_OOM, "cudaMalloc robot tables: %s", cudaGetErrorString(e));
+        }
+        e = cudaMemcpy(R->d_blob[f], blob.data(), blob.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            ik_robot_destroy(R);
+            return fail(IK_E_CUDA, "copy robot tables: %s", cudaGetErrorString(e));
+        }
+    }
+    *out = R;
+    return IK_OK;
+}
+
+int ik_robot_destroy(IkRobot* robot) {
+    if (!robot) return IK_OK;
+    for (int f = 0; f < 2; ++f)
+        if (robot->d_blob[f]) cudaFree(robot->d_blob[f]);
+    delete robot;
+    return IK_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int build_problem_blob(IkProblem* P) {
+    const RobotHost& r = P->robot->h;
+    BlobBuilder b;
+    add_robot_tables(b, r);
+    TabHeader* h = b.hdr();
+    const int boff = P->floating ? 6 : 0;
+    h->D = boff + r.na;
+    h->base_off = boff;
+    h->T = h->D * (h->D + 1) / 2;
+    h->E = h->T + h->D;
+    h->Dp = h->D;
+    h->mask_any = P->mask_any;
+    h->R_ref = P->R;
+    // pose entries
+    std::vector<PoseEntry> pose;
+    std::vector<CollEntry> coll;
+    std::vector<float> limw(std::max(r.na, 1), 0.f);
+    int has_limit = 0, limit_row = 0;
+    for (size_t ti = 0; ti < P->terms.size(); ++ti) {
+        const TermHost& th = P->terms[ti];
+        const int kind = th.d.kind;
+        if (kind == IK_TERM_POSITION || kind == IK_TERM_ROTATION) {
+            for (int f = 0; f < th.d.num_frames; ++f) {
+                PoseEntry e;
+                std::memset(&e, 0, sizeof(e));
+                e.link = th.frame_links[f];
+                e.kind = kind == IK_TERM_POSITION ? kPosePosition : kPoseRotation;
+                e.term = (int)ti;
+                e.frame = f;
+                e.num_frames = th.d.num_frames;
+                e.out_row = th.row + 3 * f;
+                e.target_rows = th.d.target_rows;
+                for (int k = 0; k < 3; ++k) e.w[k] = th.weights[3 * f + k];
+                e.targets = th.d.d_targets;
+                pose.push_back(e);
+            }
+        } else if (kind == IK_TERM_POSITION_LIMIT) {
+            has_limit = 1;
+            limit_row = th.row;
+            for (int a = 0; a < r.na; ++a) limw[a] = th.weights[a];
+        }
+    }
+    h = b.hdr();
+    h->npose = (int)pose.size();
+    h->has_limit = has_limit;
+    h->limit_row = limit_row;
+    // collision arrays
+    int slot_bytes = 0;
+    std::vector<int> coll_slot_rel;
+    for (size_t ti = 0; ti < P->terms.size(); ++ti) {
+        const TermHost& th = P->terms[ti];
+        if (th.d.kind != IK_TERM_SELF_COLLISION) continue;
+        CollEntry c;
+        std::memset(&c, 0, sizeof(c));
+        c.mode = th.d.pair_mode;
+        c.K = th.d.max_active_pairs;
+        c.nlp = th.d.num_link_pairs;
+        c.nsp = th.d.num_sphere_pairs;
+        c.out_row = th.row;
+        c.rows = th.rows;
+        c.margin = th.d.margin;
+        c.weight = th.weights[0];
+        c.o_lp = b.addv(th.lp);
+        c.o_lpoff = b.addv(th.lpoff);
+        c.o_sp = b.addv(th.sp);
+        coll_slot_rel.push_back(slot_bytes);
+        if (c.mode == IK_PAIRS_SLOTS) slot_bytes += al16(std::min(c.K, std::max(c.nlp, 1)) * (int)sizeof(Slot));
+        coll.push_back(c);
+    }
+    int max_slots = 0;
+    for (auto& c : coll)
+        if (c.mode == IK_PAIRS_SLOTS) max_slots += std::min(c.K, c.nlp);
+    int o = b.add(pose.data(), pose.size() * sizeof(PoseEntry));
+    b.hdr()->o_pose = o;
+    const int o_coll = b.add(coll.data(), coll.size() * sizeof(CollEntry));
+    b.hdr()->o_coll = o_coll;
+    o = b.addv(limw);
+    b.hdr()->o_limw = o;
+    std::vector<float> mask = P->mask;
+    if (mask.empty()) mask.assign(b.hdr()->D, 1.f);
+    o = b.addv(mask);
+    b.hdr()->o_mask = o;
+    std::vector<uint16_t> ab = ab_table(b.hdr()->D);
+    o = b.addv(ab);
+    b.hdr()->o_ab = o;
+    h = b.hdr();
+    h->ncoll = (int)coll.size();
+    h->max_slots = max_slots;
+    const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0, max_slots > 0);
+    CollEntry* ce = reinterpret_cast<CollEntry*>(b.buf.data() + o_coll);
+    for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
+    h->bytes = (int)b.buf.size();
+    P->blob = b.buf;
+    P->blob_bytes = h->bytes;
+    P->ws_bytes = h->ws_bytes;
+    P->E = h->E;
+    return IK_OK;
+}
+
+int upload_blob(IkProblem* P, void* stream) {
+    if (!P->d_blob) {
+        cudaError_t e = cudaMalloc(&P->d_blob, P->blob.size());
+        if (e != cudaSuccess) return fail(IK_E_OOM, "cudaMalloc tables: %s", cudaGetErrorString(e));
+    }
+    if (stream)
+        CK(cudaMemcpyAsync(P->d_blob, P->blob.data(), P->blob.size(), cudaMemcpyHostToDevice, S(stream)));
+    else
+        CK(cudaMemcpy(P->d_blob, P->blob.data(), P->blob.size(), cudaMemcpyHostToDevice));
+    return IK_OK;
+}
+
+int problem_group(const IkProblem* P) {
+    return choose_group(P->D, P->blob_bytes, P->ws_bytes, P->group);
+}
+
+int check_batch(const IkProblem* P, int batch) {
+    if (!P) return fail(IK_E_INVALID, "problem is NULL");
+    if (batch < 0) return fail(IK_E_INVALID, "batch %d < 0", batch);
+    if (batch > P->capacity)
+        return fail(IK_E_CAPACITY, "batch size %d exceeds the %d this optimizer was built for", batch, P->capacity);
+    return IK_OK;
+}
+
+int check_params(const IkLmParams* p) {
+    if (!p) return fail(IK_E_INVALID, "params is NULL");
+    if (!(p->lambda_factor > 0.f) || !(p->lambda_min >= 0.f) || !(p->lambda_max >= p->lambda_min))
+        return fail(IK_E_INVALID, "damping parameters are inconsistent");
+    if (p->max_iter < 0) return fail(IK_E_INVALID, "max_iter < 0");
+    return IK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ik_problem_create(IkRobot* robot, int32_t capacity, int32_t floating_base, const IkTermDesc* terms,
+                      int32_t num_terms, const float* active_dof_mask, IkProblem** out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!robot) return fail(IK_E_INVALID, "robot is NULL");
+    if (capacity < 1) return fail(IK_E_INVALID, "capacity %d < 1", capacity);
+    if (num_terms < 0 || (num_terms > 0 && !terms)) return fail(IK_E_INVALID, "terms array is NULL");
+    const RobotHost& r = robot->h;
+    const int D = (floating_base ? 6 : 0) + r.na;
+    if (D > kMaxDim) return fail(IK_E_UNSUPPORTED, "tangent dimension %d exceeds %d", D, kMaxDim);
+    if (D < 1) return fail(IK_E_INVALID, "tangent dimension is 0");
+    IkProblem* P = new IkProblem();
+    P->robot = robot;
+    P->capacity = capacity;
+    P->floating = floating_base ? 1 : 0;
+    P->D = D;
+    int row = 0, nlimit = 0;
+    for (int i = 0; i < num_terms; ++i) {
+        const IkTermDesc& d = terms[i];
+        TermHost th;
+        th.d = d;
+        th.row = row;
+        if (d.kind == IK_TERM_POSITION || d.kind == IK_TERM_ROTATION) {
+            if (d.num_frames < 1 || !d.frame_links || !d.weights) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: pose term needs frames and weights", i);
+            }
+            if (!d.d_targets) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: pose term needs a target array", i);
+            }
+            th.frame_links.assign(d.frame_links, d.frame_links + d.num_frames);
+            for (int f : th.frame_links)
+                if (f < 0 || f >= r.nl) {
+                    delete P;
+                    return fail(IK_E_INVALID, "term %d: frame link %d out of range", i, f);
+                }
+            th.weights.assign(d.weights, d.weights + 3 * d.num_frames);
+            th.rows = 3 * d.num_frames;
+        } else if (d.kind == IK_TERM_POSITION_LIMIT) {
+            if (++nlimit > 1) {
+                delete P;
+                return fail(IK_E_UNSUPPORTED, "more than one PositionLimit term");
+            }
+            if (!d.weights && r.na > 0) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: limit weights are NULL", i);
+            }
+            th.weights.assign(d.weights, d.weights + r.na);
+            th.rows = r.na;
+        } else if (d.kind == IK_TERM_SELF_COLLISION) {
+            if (r.ns < 2) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: robot has no collision spheres", i);
+            }
+            if (d.pair_mode != IK_PAIRS_SLOTS && d.pair_mode != IK_PAIRS_ALL) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: pair_mode %d", i, d.pair_mode);
+            }
+            if (d.pair_mode == IK_PAIRS_SLOTS && d.max_active_pairs < 1) {
+                delete P;
+                return fail(IK_E_INVALID, "max_active_pairs must be >= 1.");
+            }
+            if (!d.weights) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: weight is NULL", i);
+            }
+            th.weights.assign(d.weights, d.weights + 1);
+            if (d.num_link_pairs < 0 || d.num_sphere_pairs < 0 ||
+                (d.num_link_pairs > 0 && (!d.link_pairs || !d.link_pair_offsets || !d.sphere_pairs))) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: pair tables are inconsistent", i);
+            }
+            th.lp.assign(d.link_pairs, d.link_pairs + 2 * d.num_link_pairs);
+            th.lpoff.assign(d.link_pair_offsets, d.link_pair_offsets + d.num_link_pairs + 1);
+            if (d.num_link_pairs == 0) th.lpoff.assign(1, 0);
+            if (th.lpoff.front() != 0 || th.lpoff.back() != d.num_sphere_pairs) {
+                delete P;
+                return fail(IK_E_INVALID, "term %d: link pair offsets do not cover the sphere pairs", i);
+            }
+            for (int k = 0; k < d.num_link_pairs; ++k) {
+                if (th.lpoff[k + 1] < th.lpoff[k]) {
+                    delete P;
+                    return fail(IK_E_INVALID, "term %d: link pair offsets decrease", i);
+                }
+                for (int s = 0; s < 2; ++s)
+                    if (th.lp[2 * k + s] < 0 || th.lp[2 * k + s] >= r.nl) {
+                        delete P;
+                        return fail(IK_E_INVALID, "term %d: link pair %d out of range", i, k);
+                    }
+            }
+            th.sp.resize(d.num_sphere_pairs);
+            for (int k = 0; k < d.num_sphere_pairs; ++k) {
+                const int a = d.sphere_pairs[2 * k], b = d.sphere_pairs[2 * k + 1];
+                if (a < 0 || a >= r.ns || b < 0 || b >= r.ns) {
+                    delete P;
+                    return fail(IK_E_INVALID, "term %d: sphere pair %d out of range", i, k);
+                }
+                th.sp[k] = a | (b << 16);
+            }
+            th.rows = d.pair_mode == IK_PAIRS_SLOTS ? d.max_active_pairs : d.num_sphere_pairs;
+        } else {
+            delete P;
+            return fail(IK_E_INVALID, "term %d: unknown kind %d", i, d.kind);
+        }
+        row += th.rows;
+        P->terms.push_back(th);
+    }
+    P->R = row;
+    if (active_dof_mask) {
+        P->mask.assign(active_dof_mask, active_dof_mask + D);
+        for (float m : P->mask)
+            if (m != 1.f) P->mask_any = 1;
+    }
+    int rc = build_problem_blob(P);
+    if (!rc) rc = upload_blob(P, nullptr);
+    if (!rc) {
+        const int rs = rec_stride(P->E);
+        cudaError_t e = cudaMalloc(&P->d_rec, (size_t)capacity * rs * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&P->d_counters, 8 * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&P->d_queue, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(P->d_counters, 0, 8 * sizeof(int));
+        if (e != cudaSuccess) rc = fail(IK_E_OOM, "problem buffers: %s", cudaGetErrorString(e));
+    }
+    if (!rc) {
+        const int G = problem_group(P);
+        if (smem_bytes(P->blob_bytes, P->ws_bytes, G) > max_smem_optin())
+            rc = fail(IK_E_UNSUPPORTED, "problem needs %d B of shared memory per block",
+                      smem_bytes(P->blob_bytes, P->ws_bytes, G));
+    }
+    if (rc) {
+        ik_problem_destroy(P);
+        return rc;
+    }
+    *out = P;
+    return IK_OK;
+}
+
+int ik_problem_destroy(IkProblem* P) {
+    if (!P) return IK_OK;
+    if (P->d_blob) cudaFree(P->d_blob);
+    if (P->d_rec) cudaFree(P->d_rec);
+    if (P->d_counters) cudaFree(P->d_counters);
+    if (P->d_queue) cudaFree(P->d_queue);
+    delete P;
+    return IK_OK;
+}
+
+int ik_problem_info(const IkProblem* P, int32_t* tangent_dim, int32_t* residual_dim, int32_t* capacity) {
+    if (!P) return fail(IK_E_INVALID, "problem is NULL");
+    if (tangent_dim) *tangent_dim = P->D;
+    if (residual_dim) *residual_dim = P->R;
+    if (capacity) *capacity = P->capacity;
+    return IK_OK;
+}
+
+int ik_problem_set_targets(IkProblem* P, int32_t term_index, const float* d_targets, int32_t target_rows) {
+    if (!P) return fail(IK_E_INVALID, "problem is NULL");
+    if (term_index < 0 || term_index >= (int)P->terms.size()) return fail(IK_E_INVALID, "term %d out of range", term_index);
+    TermHost& th = P->terms[term_index];
+    if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION)
+        return fail(IK_E_INVALID, "term %d has no pose targets", term_index);
+    if (!d_targets) return fail(IK_E_INVALID, "targets are NULL");
+    th.d.d_targets = d_targets;
+    th.d.target_rows = target_rows;
+    int rc = build_problem_blob(P);
+    if (rc) return rc;
+    return upload_blob(P, nullptr);
+}
+
+int ik_problem_set_schedule(IkProblem* P, int32_t group_lanes, int32_t blocks_per_sm) {
+    if (!P) return fail(IK_E_INVALID, "problem is NULL");
+    if (group_lanes != 0 && group_lanes != 8 && group_lanes != 16 && group_lanes != 32)
+        return fail(IK_E_INVALID, "group_lanes %d not in {0, 8, 16, 32}", group_lanes);
+    if (blocks_per_sm < 0) return fail(IK_E_INVALID, "blocks_per_sm < 0");
+    if (group_lanes && smem_bytes(P->blob_bytes, P->ws_bytes, group_lanes) > max_smem_optin())
+        return fail(IK_E_UNSUPPORTED, "group width %d needs too much shared memory", group_lanes);
+    P->group = group_lanes;
+    P->blocks_per_sm = blocks_per_sm;
+    return IK_OK;
+}
+
+int ik_problem_get_schedule(const IkProblem* P, int32_t* group_lanes, int32_t* blocks_per_sm) {
+    if (!P) return fail(IK_E_INVALID, "problem is NULL");
+    if (group_lanes) *group_lanes = problem_group(P);
+    if (blocks_per_sm) *blocks_per_sm = P->blocks_per_sm;
+    return IK_OK;
+}
+
+int ik_solve_plain(IkProblem* P, int32_t batch, float* d_q, float* d_base, const IkLmParams* params, float* d_cost,
+                   float* d_lambda, int32_t* d_iters, int32_t* d_status, void* stream) {
+    int rc = check_batch(P, batch);
+    if (rc) return rc;
+    rc = check_params(params);
+    if (rc) return rc;
+    if (!d_q && P->robot->h.na > 0) return fail(IK_E_INVALID, "q is NULL");
+    if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
+    if (batch == 0) return IK_OK;
+    const int G = problem_group(P);
+    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
+    const IkLmParams prm = *params;
+    IK_DISPATCH(G, lm_plain_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid);
+        if (rc) return rc;
+        for (int k = -1; k < prm.max_iter; ++k) {
+            kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, P->d_rec, prm,
+                                                          k < 0 ? 0 : 1, k < 0 ? 0 : k, P->d_counters, d_cost,
+                                                          d_lambda, d_iters, d_status);
+            rc = check_launch();
+            if (rc) return rc;
+        }
+    });
+    return IK_OK;
+}
+
+int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, const IkLmParams* params,
+                        float* d_cost, float* d_lambda, int32_t* d_iters, int32_t* d_status, void* stream) {
+    int rc = check_batch(P, batch);
+    if (rc) return rc;
+    rc = check_params(params);
+    if (rc) return rc;
+    if (params->stop_rules & IK_STOP_ALL_COST)
+        return fail(IK_E_INVALID, "the all-problems cost rule needs the plain form");
+    if (!d_q && P->robot->h.na > 0) return fail(IK_E_INVALID, "q is NULL");
+    if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
+    if (batch == 0) return IK_OK;
+    const int G = problem_group(P);
+    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
+    const IkLmParams prm = *params;
+    CK(cudaMemsetAsync(P->d_queue, 0, sizeof(int), S(stream)));
+    IK_DISPATCH(G, lm_persistent_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, prm, P->d_queue, d_cost,
+                                                      d_lambda, d_iters, d_status);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_fk(IkRobot* R, int32_t batch, const float* d_q, const float* d_base, float* d_T_joint, float* d_T_link,
+          float* d_S_world, float* d_spheres, float* d_link_bounds, void* stream) {
+    if (!R) return fail(IK_E_INVALID, "robot is NULL");
+    if (batch < 0) return fail(IK_E_INVALID, "batch < 0");
+    if (batch == 0) return IK_OK;
+    if (!d_q && R->h.na > 0) return fail(IK_E_INVALID, "q is NULL");
+    const int f = d_base ? 1 : 0;
+    const int D = (f ? 6 : 0) + R->h.na;
+    const int G = choose_group(D, R->blob_bytes[f], R->ws_bytes[f], 0);
+    const int smem = smem_bytes(R->blob_bytes[f], R->ws_bytes[f], G);
+    int rc = 0;
+    IK_DISPATCH(G, fk_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(R->d_blob[f], batch, d_q, d_base, d_T_joint, d_T_link,
+                                                      d_S_world, d_spheres, d_link_bounds);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_link_jacobian(IkRobot* R, int32_t batch, const float* d_q, const float* d_base, int32_t link,
+                     int32_t body_frame, float* d_J, void* stream) {
+    if (!R) return fail(IK_E_INVALID, "robot is NULL");
+    if (batch < 0) return fail(IK_E_INVALID, "batch < 0");
+    if (link < 0 || link >= R->h.nl) return fail(IK_E_INVALID, "link %d out of range", link);
+    if (!d_J) return fail(IK_E_INVALID, "output is NULL");
+    if (batch == 0) return IK_OK;
+    const int f = d_base ? 1 : 0;
+    const int D = (f ? 6 : 0) + R->h.na;
+    const int G = choose_group(D, R->blob_bytes[f], R->ws_bytes[f], 0);
+    const int smem = smem_bytes(R->blob_bytes[f], R->ws_bytes[f], G);
+    int rc = 0;
+    IK_DISPATCH(G, link_jacobian_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(R->d_blob[f], batch, d_q, d_base, link, body_frame ? 1 : 0,
+                                                      d_J);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_residual_jacobian(IkProblem* P, int32_t batch, const float* d_q, const float* d_base, float* d_r, float* d_J,
+                         void* stream) {
+    int rc = check_batch(P, batch);
+    if (rc) return rc;
+    if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
+    if (batch == 0) return IK_OK;
+    if (d_r) CK(cudaMemsetAsync(d_r, 0, (size_t)batch * P->R * sizeof(float), S(stream)));
+    if (d_J) CK(cudaMemsetAsync(d_J, 0, (size_t)batch * P->R * P->D * sizeof(float), S(stream)));
+    const int G = problem_group(P);
+    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
+    IK_DISPATCH(G, resjac_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, d_r, d_J);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_normal_equations(IkProblem* P, int32_t batch, const float* d_q, const float* d_base, float* d_H, float* d_g,
+                        float* d_cost, void* stream) {
+    int rc = check_batch(P, batch);
+    if (rc) return rc;
+    if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
+    if (batch == 0) return IK_OK;
+    const int G = problem_group(P);
+    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
+    IK_DISPATCH(G, normal_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, d_H, d_g, d_cost);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_damped_solve(int32_t batch, int32_t dim, const float* d_H, const float* d_g, const float* d_lambda,
+                    float* d_delta, float* d_pred, int32_t* d_spd, void* stream) {
+    if (batch < 0) return fail(IK_E_INVALID, "batch < 0");
+    if (dim < 1 || dim > kMaxDim) return fail(IK_E_UNSUPPORTED, "dimension %d outside [1, %d]", dim, kMaxDim);
+    if (!d_H || !d_g || !d_lambda || !d_delta || !d_pred) return fail(IK_E_INVALID, "NULL array");
+    if (batch == 0) return IK_OK;
+    // a table blob that carries only the dimension and its entry table
+    static thread_local std::vector<char*> cache(kMaxDim + 1, nullptr);
+    static thread_local std::vector<int> cache_bytes(kMaxDim + 1, 0), cache_ws(kMaxDim + 1, 0);
+    if (!cache[dim]) {
+        RobotHost r;
+        r.na = dim;
+        r.nj = 0;
+        r.nl = 1;
+        r.lpj.assign(1, -1);
+        r.lanc.assign(1, 0ull);
+        r.lbound.assign(4, 0.f);
+        r.lim.assign(2 * dim, 0.f);
+        r.colstart.assign(dim + 1, 0);
+        r.coljoint.assign(1, 0);
+        r.colmul.assign(1, 0.f);
+        std::vector<char> blob;
+        int ws = 0;
+        build_robot_blob(r, 0, blob, ws);
+        char* d = nullptr;
+        CK(cudaMalloc(&d, blob.size()));
+        CK(cudaMemcpy(d, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+        cache[dim] = d;
+        cache_bytes[dim] = (int)blob.size();
+        cache_ws[dim] = ws;
+    }
+    const int G = choose_group(dim, cache_bytes[dim], cache_ws[dim], 0);
+    const int smem = smem_bytes(cache_bytes[dim], cache_ws[dim], G);
+    int rc = 0;
+    IK_DISPATCH(G, damped_solve_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(cache[dim], batch, d_H, d_g, d_lambda, d_delta, d_pred, d_spd);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_step(IkProblem* P, int32_t batch, float* d_q, float* d_base, float* d_lambda, const IkLmParams* params,
+            float* d_cost, float* d_delta, float* d_pred, float* d_cost_new, int32_t* d_accept, void* stream) {
+    int rc = check_batch(P, batch);
+    if (rc) return rc;
+    rc = check_params(params);
+    if (rc) return rc;
+    if (!d_lambda) return fail(IK_E_INVALID, "lambda is NULL");
+    if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
+    if (batch == 0) return IK_OK;
+    const int G = problem_group(P);
+    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
+    const IkLmParams prm = *params;
+    IK_DISPATCH(G, step_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, d_lambda, prm, d_cost, d_delta,
+                                                      d_pred, d_cost_new, d_accept);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_accept_reject(int32_t batch, float* d_cost, const float* d_cost_new, const float* d_pred, float* d_lambda,
+                     int32_t* d_accept, const IkLmParams* params, void* stream) {
+    if (batch < 0) return fail(IK_E_INVALID, "batch < 0");
+    int rc = check_params(params);
+    if (rc) return rc;
+    if (!d_cost || !d_cost_new || !d_pred || !d_lambda || !d_accept) return fail(IK_E_INVALID, "NULL array");
+    if (batch == 0) return IK_OK;
+    accept_kernel<<<(batch + 127) / 128, 128, 0, S(stream)>>>(batch, d_cost, d_cost_new, d_pred, d_lambda, d_accept,
+                                                              *params);
+    return check_launch();
+}
+
+int ik_metrics(IkRobot* R, int32_t batch, const float* d_q, const float* d_base, int32_t num_targets,
+               const int32_t* d_target_links, const float* d_targets, float pos_threshold, float rot_threshold,
+               float* d_pos_err, float* d_rot_err, int32_t* d_success, void* stream) {
+    if (!R) return fail(IK_E_INVALID, "robot is NULL");
+    if (batch < 0 || num_targets < 1) return fail(IK_E_INVALID, "batch < 0 or no targets");
+    if (!d_target_links || !d_targets || !d_pos_err || !d_rot_err || !d_success)
+        return fail(IK_E_INVALID, "NULL array");
+    if (batch == 0) return IK_OK;
+    const int f = d_base ? 1 : 0;
+    const int D = (f ? 6 : 0) + R->h.na;
+    const int G = choose_group(D, R->blob_bytes[f], R->ws_bytes[f], 0);
+    const int smem = smem_bytes(R->blob_bytes[f], R->ws_bytes[f], G);
+    int rc = 0;
+    IK_DISPATCH(G, metrics_kernel, {
+        rc = prepare_kernel(kfn, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        if (rc) return rc;
+        kfn<<<grid, kBlockThreads, smem, S(stream)>>>(R->d_blob[f], batch, d_q, d_base, num_targets, d_target_links,
+                                                      d_targets, pos_threshold, rot_threshold, d_pos_err, d_rot_err,
+                                                      d_success);
+        rc = check_launch();
+        if (rc) return rc;
+    });
+    return IK_OK;
+}
+
+int ik_integrate(int32_t batch, int32_t num_actuated, int32_t floating_base, const float* d_q, const float* d_base,
+                 const float* d_delta, const float* d_mask, float* d_q_out, float* d_base_out, void* stream) {
+    if (batch < 0 || num_actuated < 0) return fail(IK_E_INVALID, "negative size");
+    if (!d_q || !d_delta || !d_q_out) return fail(IK_E_INVALID, "NULL array");
+    if (floating_base && (!d_base || !d_base_out)) return fail(IK_E_INVALID, "base arrays are NULL");
+    if (batch == 0) return IK_OK;
+    integrate_kernel<<<(batch + 127) / 128, 128, 0, S(stream)>>>(batch, num_actuated, floating_base ? 1 : 0, d_q,
+                                                                 d_base, d_delta, d_mask, d_q_out, d_base_out);
+    return check_launch();
+}
+
+static int elementwise_grid(long long n) {
+    long long g = (n + 255) / 256;
+    if (g < 1) g = 1;
+    if (g > 65535) g = 65535;
+    return (int)g;
+}
+
+int ik_copy_rows(int32_t rows, int32_t width, const float* d_src, int64_t src_stride, float* d_dst, int64_t dst_stride,
+                 void* stream) {
+    if (rows < 0 || width < 0) return fail(IK_E_INVALID, "negative size");
+    if (rows == 0 || width == 0) return IK_OK;
+    if (!d_src || !d_dst) return fail(IK_E_INVALID, "NULL array");
+    copy_rows_kernel<<<elementwise_grid((long long)rows * width), 256, 0, S(stream)>>>(rows, width, d_src, src_stride,
+                                                                                        d_dst, dst_stride);
+    return check_launch();
+}
+
+int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, const float* d_src, float* d_dst,
+                        void* stream) {
+    if (rows < 0 || width < 0) return fail(IK_E_INVALID, "negative size");
+    if (rows == 0 || width == 0) return IK_OK;
+    if (!d_mask || !d_src || !d_dst) return fail(IK_E_INVALID, "NULL array");
+    masked_copy_rows_kernel<<<elementwise_grid((long long)rows * width), 256, 0, S(stream)>>>(rows, width, d_mask,
+                                                                                               d_src, d_dst);
+    return check_launch();
+}
+
+int ik_clamp_q(int32_t batch, int32_t num_actuated, float* d_q, const float* d_limits, const float* d_mask,
+               void* stream) {
+    if (batch < 0 || num_actuated < 0) return fail(IK_E_INVALID, "negative size");
+    if (batch == 0 || num_actuated == 0) return IK_OK;
+    if (!d_q || !d_limits) return fail(IK_E_INVALID, "NULL array");
+    clamp_q_kernel<<<elementwise_grid((long long)batch * num_actuated), 256, 0, S(stream)>>>(batch, num_actuated, d_q,
+                                                                                             d_limits, d_mask);
+    return check_launch();
+}
+
+// ---- memory / streams / events -------------------------------------------------
+int ik_malloc(void** p, size_t bytes) {
+    if (!p) return fail(IK_E_INVALID, "out is NULL");
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail(IK_E_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    return IK_OK;
+}
+int ik_free(void* p) {
+    if (p) CK(cudaFree(p));
+    return IK_OK;
+}
+int ik_malloc_host(void** p, size_t bytes) {
+    if (!p) return fail(IK_E_INVALID, "out is NULL");
+    cudaError_t e = cudaMallocHost(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail(IK_E_OOM, "cudaMallocHost(%zu): %s", bytes, cudaGetErrorString(e));
+    return IK_OK;
+}
+int ik_free_host(void* p) {
+    if (p) CK(cudaFreeHost(p));
+    return IK_OK;
+}
+int ik_memcpy_htod(void* d, const void* h, size_t bytes, void* stream) {
+    if (bytes == 0) return IK_OK;
+    CK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, S(stream)));
+    return IK_OK;
+}
+int ik_memcpy_dtoh(void* h, const void* d, size_t bytes, void* stream) {
+    if (bytes == 0) return IK_OK;
+    CK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, S(stream)));
+    return IK_OK;
+}
+int ik_memcpy_dtod(void* d, const void* s, size_t bytes, void* stream) {
+    if (bytes == 0) return IK_OK;
+    CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, S(stream)));
+    return IK_OK;
+}
+int ik_memset(void* d, int value, size_t bytes, void* stream) {
+    if (bytes == 0) return IK_OK;
+    CK(cudaMemsetAsync(d, value, bytes, S(stream)));
+    return IK_OK;
+}
+int ik_stream_create(void** stream) {
+    if (!stream) return fail(IK_E_INVALID, "out is NULL");
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *stream = s;
+    return IK_OK;
+}
+int ik_stream_destroy(void* stream) {
+    if (stream) CK(cudaStreamDestroy(S(stream)));
+    return IK_OK;
+}
+int ik_stream_synchronize(void* stream) {
+    CK(cudaStreamSynchronize(S(stream)));
+    return IK_OK;
+}
+int ik_device_synchronize(void) {
+    CK(cudaDeviceSynchronize());
+    return IK_OK;
+}
+int ik_event_create(void** ev) {
+    if (!ev) return fail(IK_E_INVALID, "out is NULL");
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    *ev = e;
+    return IK_OK;
+}
+int ik_event_destroy(void* ev) {
+    if (ev) CK(cudaEventDestroy(reinterpret_cast<cudaEvent_t>(ev)));
+    return IK_OK;
+}
+int ik_event_record(void* ev, void* stream) {
+    CK(cudaEventRecord(reinterpret_cast<cudaEvent_t>(ev), S(stream)));
+    return IK_OK;
+}
+int ik_event_elapsed_ms(void* a, void* b, float* ms) {
+    if (!ms) return fail(IK_E_INVALID, "out is NULL");
+    CK(cudaEventElapsedTime(ms, reinterpret_cast<cudaEvent_t>(a), reinterpret_cast<cudaEvent_t>(b)));
+    return IK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,947 @@
+// ik_device.cuh — device routines of the fused LM-IK kernel.
+//
+// A *group* of G lanes (G = 8, 16 or 32, always inside one warp) owns one IK
+// problem.  The routines below are written for the group: loops over joints,
+// residual rows, normal-equation entries and Cholesky items are strided by the
+// group lane, synchronisation is __syncwarp on the group's lane mask and
+// reductions are width-G shuffles.  Tables come from the staged blob
+// (ik_tables.h); the per-group workspace is a private slice of shared memory.
+//
+// Numerics: kinematics, residuals, the Jacobian and J^T J run in FP32; J^T J,
+// J^T r and the cost use compensated (Neumaier/Kahan) accumulation across row
+// chunks; the damped Cholesky factorisation, the solve, the predicted
+// reduction and the gain ratio run in FP64.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "ik_tables.h"
+
+namespace b200ik {
+
+// ---------------------------------------------------------------------------
+// SE(3) on [x y z | qw qx qy qz] poses (lie/se3_kernels.py:70-167,324-346,
+// xform/warp/rotation_conversions.py:169-279).  Quaternion products are
+// standardised to w >= 0 like quaternion_multiply_func (:268-279).
+// ---------------------------------------------------------------------------
+struct Pose {
+    float x, y, z, w, i, j, k;
+};
+
+__device__ __forceinline__ Pose pose_identity() { return Pose{0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f}; }
+
+__device__ __forceinline__ Pose pose_load(const float* p) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    const float4 b = *reinterpret_cast<const float4*>(p + 4);
+    return Pose{a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+}
+__device__ __forceinline__ void pose_store(float* p, const Pose& P) {
+    *reinterpret_cast<float4*>(p) = make_float4(P.x, P.y, P.z, P.w);
+    *reinterpret_cast<float4*>(p + 4) = make_float4(P.i, P.j, P.k, 0.f);
+}
+__device__ __forceinline__ Pose pose_load7(const float* p) {  // unaligned 7-float pose
+    return Pose{p[0], p[1], p[2], p[3], p[4], p[5], p[6]};
+}
+
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator*(float s, V3 a) { return V3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ float norm3(V3 a) { return sqrtf(dot(a, a)); }
+
+// v' = v + 2 (w (u x v) + u x (u x v)), quaternion_apply_func :192-200
+__device__ __forceinline__ V3 qrot(float w, float i, float j, float k, V3 v) {
+    const V3 u{i, j, k};
+    const V3 uv = cross(u, v);
+    const V3 uuv = cross(u, uv);
+    return v + 2.0f * (w * uv + uuv);
+}
+__device__ __forceinline__ V3 pose_apply(const Pose& P, V3 v) { return qrot(P.w, P.i, P.j, P.k, v) + V3{P.x, P.y, P.z}; }
+
+__device__ __forceinline__ void qmul_std(float aw, float ai, float aj, float ak, float bw, float bi, float bj, float bk,
+                                         float& w, float& i, float& j, float& k) {
+    w = aw * bw - ai * bi - aj * bj - ak * bk;
+    i = aw * bi + ai * bw + aj * bk - ak * bj;
+    j = aw * bj - ai * bk + aj * bw + ak * bi;
+    k = aw * bk + ai * bj - aj * bi + ak * bw;
+    if (w < 0.f) {
+        w = -w;
+        i = -i;
+        j = -j;
+        k = -k;
+    }
+}
+
+// A o B, se3_compose_func :88-109
+__device__ __forceinline__ Pose compose(const Pose& A, const Pose& B) {
+    Pose O;
+    qmul_std(A.w, A.i, A.j, A.k, B.w, B.i, B.j, B.k, O.w, O.i, O.j, O.k);
+    const V3 t = qrot(A.w, A.i, A.j, A.k, V3{B.x, B.y, B.z});
+    O.x = A.x + t.x;
+    O.y = A.y + t.y;
+    O.z = A.z + t.z;
+    return O;
+}
+
+// SE(3) exponential with regularised angle, se3_exp_map_func :126-167
+__device__ __forceinline__ Pose se3_exp(const float xi[6], float eps) {
+    const V3 tl{xi[0], xi[1], xi[2]};
+    const V3 rl{xi[3], xi[4], xi[5]};
+    const float angle_sq = dot(rl, rl);
+    const float angle_sq_reg = angle_sq + eps * eps;
+    const float angle_reg = sqrtf(angle_sq_reg);
+    float sh, ch;
+    sincosf(angle_reg * 0.5f, &sh, &ch);
+    const float kk = sh / angle_reg;
+    float qw = ch, qi = kk * rl.x, qj = kk * rl.y, qk = kk * rl.z;
+    const float qn = sqrtf(qw * qw + qi * qi + qj * qj + qk * qk);
+    qw /= qn;
+    qi /= qn;
+    qj /= qn;
+    qk /= qn;
+    float sa, ca;
+    sincosf(angle_reg, &sa, &ca);
+    const float A = sa / angle_reg;
+    const float c1 = (1.0f - ca) / angle_sq_reg;
+    const float c2 = (1.0f - A) / angle_sq_reg;
+    // V = I + c1 K + c2 K^2 with K = hat(rl); V t = t + c1 (rl x t) + c2 (rl x (rl x t))
+    const V3 kt = cross(rl, tl);
+    const V3 kkt = cross(rl, kt);
+    const V3 tr = tl + c1 * kt + c2 * kkt;
+    return Pose{tr.x, tr.y, tr.z, qw, qi, qj, qk};
+}
+
+// axis-angle of a standardised quaternion, quaternion_to_axis_angle_func :228-247
+__device__ __forceinline__ V3 quat_to_axis_angle(float w, float i, float j, float k) {
+    const float n = sqrtf(i * i + j * j + k * k);
+    const float half = atan2f(n, w);
+    const float angle = 2.0f * half;
+    float s;
+    if (fabsf(angle) < 1e-6f) {
+        s = 0.5f - angle * angle / 48.0f;
+    } else {
+        s = sinf(half) / angle;
+    }
+    return V3{i / s, j / s, k / s};
+}
+
+// ---------------------------------------------------------------------------
+// compensated accumulation (Neumaier's variant of Kahan summation)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void kadd(float& s, float& c, float x) {
+    const float t = s + x;
+    if (fabsf(s) >= fabsf(x))
+        c += (s - t) + x;
+    else
+        c += (x - t) + s;
+    s = t;
+}
+
+// ---------------------------------------------------------------------------
+// lane group
+// ---------------------------------------------------------------------------
+template <int G>
+struct Group {
+    int lane;       // 0..G-1
+    int wbase;      // first warp lane of this group
+    unsigned mask;  // warp lanes of this group
+    __device__ __forceinline__ Group() {
+        const int wl = threadIdx.x & 31;
+        lane = wl & (G - 1);
+        wbase = wl & ~(G - 1);
+        mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << wbase);
+    }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+    __device__ __forceinline__ float sum(float v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+        return v;
+    }
+    __device__ __forceinline__ double sumd(double v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+        return v;
+    }
+    __device__ __forceinline__ float maxf(float v) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(mask, v, o, G));
+        return v;
+    }
+    __device__ __forceinline__ int bcast(int v, int src) const { return __shfl_sync(mask, v, src, G); }
+    __device__ __forceinline__ unsigned ballot(bool p) const { return (__ballot_sync(mask, p) >> wbase) & ((G == 32) ? 0xffffffffu : ((1u << G) - 1u)); }
+    __device__ __forceinline__ unsigned lt_mask() const { return (1u << lane) - 1u; }
+};
+
+// Compensated group sum: each lane holds (s, c); the group reduces pairs.
+template <int G>
+__device__ __forceinline__ float group_ksum(const Group<G>& g, float s, float c) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        const float so = __shfl_xor_sync(g.mask, s, o, G);
+        const float co = __shfl_xor_sync(g.mask, c, o, G);
+        c += co;
+        kadd(s, c, so);
+    }
+    return s + c;
+}
+
+// ---------------------------------------------------------------------------
+// table / workspace views
+// ---------------------------------------------------------------------------
+struct Tabs {
+    const TabHeader* h;
+    const int* jtype;
+    const int* jparent;
+    const int* jact;
+    const int* jmimic;
+    const float* jmul;
+    const float* joff;
+    const float* jaxis;  // [nj*4]
+    const float* jpt;    // [nj*8]
+    const int* lpj;
+    const unsigned long long* lanc;
+    const float* lbound;  // [nl*4]
+    const float* sph;     // [ns*4]
+    const int* sphlink;
+    const float* lim;     // [na*2]
+    const int* colstart;
+    const int* coljoint;
+    const float* colmul;
+    const PoseEntry* pose;
+    const CollEntry* coll;
+    const float* limw;
+    const float* mask;
+    const uint16_t* ab;
+    const char* base;
+    __device__ __forceinline__ void bind(const char* blob) {
+        base = blob;
+        h = reinterpret_cast<const TabHeader*>(blob);
+        jtype = reinterpret_cast<const int*>(blob + h->o_jtype);
+        jparent = reinterpret_cast<const int*>(blob + h->o_jparent);
+        jact = reinterpret_cast<const int*>(blob + h->o_jact);
+        jmimic = reinterpret_cast<const int*>(blob + h->o_jmimic);
+        jmul = reinterpret_cast<const float*>(blob + h->o_jmul);
+        joff = reinterpret_cast<const float*>(blob + h->o_joff);
+        jaxis = reinterpret_cast<const float*>(blob + h->o_jaxis);
+        jpt = reinterpret_cast<const float*>(blob + h->o_jpt);
+        lpj = reinterpret_cast<const int*>(blob + h->o_lpj);
+        lanc = reinterpret_cast<const unsigned long long*>(blob + h->o_lanc);
+        lbound = reinterpret_cast<const float*>(blob + h->o_lbound);
+        sph = reinterpret_cast<const float*>(blob + h->o_sph);
+        sphlink = reinterpret_cast<const int*>(blob + h->o_sphlink);
+        lim = reinterpret_cast<const float*>(blob + h->o_lim);
+        colstart = reinterpret_cast<const int*>(blob + h->o_colstart);
+        coljoint = reinterpret_cast<const int*>(blob + h->o_coljoint);
+        colmul = reinterpret_cast<const float*>(blob + h->o_colmul);
+        pose = reinterpret_cast<const PoseEntry*>(blob + h->o_pose);
+        coll = reinterpret_cast<const CollEntry*>(blob + h->o_coll);
+        limw = reinterpret_cast<const float*>(blob + h->o_limw);
+        mask = reinterpret_cast<const float*>(blob + h->o_mask);
+        ab = reinterpret_cast<const uint16_t*>(blob + h->o_ab);
+    }
+    template <typename T>
+    __device__ __forceinline__ const T* at(int off) const { return reinterpret_cast<const T*>(base + off); }
+};
+
+struct Ws {
+    float* T0;      // FK buffer A [nj*8]
+    float* T1;      // FK buffer B [nj*8] / motion subspace
+    int* anc;       // [2*nj]
+    float* sph;     // world spheres [ns*4]
+    float* lbw;     // world link bounding centres [nl*4]
+    float* tgt;     // pose targets [npose*8]
+    float* rpose;   // pose residuals [npose*3]
+    float* rlim;    // limit residuals [na]
+    float* Jc;      // Jacobian chunk [kChunkRows*Dp]
+    float* rc;      // chunk residuals [kChunkRows]
+    float* rowmeta; // chunk row metadata [kChunkRows*8]
+    float* Hs;      // normal equations [E] (packed lower H, then g)
+    float* Hc;      // compensation terms [E]
+    double* L;      // Cholesky factor [T]
+    double* tmp;    // [D]
+    double* y;      // [D] solve vector / step
+    float* q;       // current joints [na]
+    float* qp;      // proposed joints [na]
+    float* base;    // current base pose [8]
+    float* basep;   // proposed base pose [8]
+    float* d32;     // step in FP32 [D]
+    float* misc;    // [16]
+    char* raw;
+    __device__ __forceinline__ void bind(char* w, const TabHeader* h) {
+        raw = w;
+        T0 = reinterpret_cast<float*>(w + h->w_T0);
+        T1 = reinterpret_cast<float*>(w + h->w_T1);
+        anc = reinterpret_cast<int*>(w + h->w_anc);
+        sph = reinterpret_cast<float*>(w + h->w_sph);
+        lbw = reinterpret_cast<float*>(w + h->w_lbw);
+        tgt = reinterpret_cast<float*>(w + h->w_tgt);
+        rpose = reinterpret_cast<float*>(w + h->w_rpose);
+        rlim = reinterpret_cast<float*>(w + h->w_rlim);
+        Jc = reinterpret_cast<float*>(w + h->w_Jc);
+        rc = reinterpret_cast<float*>(w + h->w_rc);
+        rowmeta = reinterpret_cast<float*>(w + h->w_rowmeta);
+        Hs = reinterpret_cast<float*>(w + h->w_Hs);
+        Hc = reinterpret_cast<float*>(w + h->w_Hc);
+        L = reinterpret_cast<double*>(w + h->w_L);
+        tmp = reinterpret_cast<double*>(w + h->w_tmp);
+        y = reinterpret_cast<double*>(w + h->w_y);
+        q = reinterpret_cast<float*>(w + h->w_q);
+        qp = reinterpret_cast<float*>(w + h->w_qp);
+        base = reinterpret_cast<float*>(w + h->w_base);
+        basep = reinterpret_cast<float*>(w + h->w_basep);
+        d32 = reinterpret_cast<float*>(w + h->w_d32);
+        misc = reinterpret_cast<float*>(w + h->w_misc);
+    }
+};
+
+// slot record of the slots-mode self-collision term: sphere pair + residual
+struct Slot {
+    int32_t i, j;
+    float r;
+    int32_t lp;
+};
+
+// ---------------------------------------------------------------------------
+// forward kinematics (robo/robot_kernels.py:265-297 local transforms,
+// :390-478 pointer jumping over the joint tree).  Returns the buffer that holds
+// T_world_joint; the other FK buffer is free afterwards.
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ float* group_fk(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
+    const int nj = t.h->nj;
+    float* src = w.T0;
+    float* dst = w.T1;
+    int* asrc = w.anc;
+    int* adst = w.anc + nj;
+    for (int j = g.lane; j < nj; j += G) {
+        float pos = 0.f;
+        const int mim = t.jmimic[j];
+        const int act = t.jact[j];
+        if (mim >= 0)
+            pos = q[mim] * t.jmul[j] + t.joff[j];
+        else if (act >= 0)
+            pos = q[act];
+        const Pose P = pose_load(t.jpt + 8 * j);
+        const int ty = t.jtype[j];
+        const float ax = t.jaxis[4 * j], ay = t.jaxis[4 * j + 1], az = t.jaxis[4 * j + 2];
+        Pose X;
+        if (ty == 2) {
+            float s, c;
+            sincosf(pos * 0.5f, &s, &c);
+            X = compose(P, Pose{0.f, 0.f, 0.f, c, ax * s, ay * s, az * s});
+        } else if (ty == 1) {
+            X = compose(P, Pose{ax * pos, ay * pos, az * pos, 1.f, 0.f, 0.f, 0.f});
+        } else {
+            X = P;
+        }
+        pose_store(src + 8 * j, X);
+        asrc[j] = t.jparent[j];
+    }
+    g.sync();
+    const int rounds = t.h->fk_rounds;
+    for (int r = 0; r < rounds; ++r) {
+        for (int j = g.lane; j < nj; j += G) {
+            const int a = asrc[j];
+            Pose X = pose_load(src + 8 * j);
+            int na = -1;
+            if (a >= 0) {
+                X = compose(pose_load(src + 8 * a), X);
+                na = asrc[a];
+            }
+            pose_store(dst + 8 * j, X);
+            adst[j] = na;
+        }
+        g.sync();
+        float* tf = src;
+        src = dst;
+        dst = tf;
+        int* ti = asrc;
+        asrc = adst;
+        adst = ti;
+    }
+    if (base != nullptr) {
+        const Pose B = pose_load(base);
+        for (int j = g.lane; j < nj; j += G) pose_store(src + 8 * j, compose(B, pose_load(src + 8 * j)));
+        g.sync();
+    }
+    return src;
+}
+
+__device__ __forceinline__ Pose link_pose(const Tabs& t, const float* Tj, const float* base, int link) {
+    const int j = t.lpj[link];
+    if (j >= 0) return pose_load(Tj + 8 * j);
+    return base ? pose_load(base) : pose_identity();
+}
+
+// world motion subspace column of joint j: [v; w] = Ad(T_world_joint) twist_j
+__device__ __forceinline__ void joint_subspace(const Tabs& t, const float* Tj, int j, V3& v, V3& om) {
+    const int ty = t.jtype[j];
+    v = V3{0.f, 0.f, 0.f};
+    om = V3{0.f, 0.f, 0.f};
+    if (ty == 0) return;
+    const Pose P = pose_load(Tj + 8 * j);
+    const V3 a{t.jaxis[4 * j], t.jaxis[4 * j + 1], t.jaxis[4 * j + 2]};
+    const V3 Ra = qrot(P.w, P.i, P.j, P.k, a);
+    if (ty == 2) {
+        om = Ra;
+        v = cross(V3{P.x, P.y, P.z}, Ra);
+    } else {
+        v = Ra;
+    }
+}
+
+// spatial column of tangent column c restricted to the ancestors of `link`
+// (position_task.py:242-249; floating-base columns :261-272).
+__device__ __forceinline__ void column_twist(const Tabs& t, const float* S, const float* base, int c, int link, V3& v,
+                                             V3& om) {
+    const int boff = t.h->base_off;
+    if (c < boff) {
+        const Pose B = pose_load(base);
+        if (c < 3) {
+            const V3 e{c == 0 ? 1.f : 0.f, c == 1 ? 1.f : 0.f, c == 2 ? 1.f : 0.f};
+            v = qrot(B.w, B.i, B.j, B.k, e);
+            om = V3{0.f, 0.f, 0.f};
+        } else {
+            const V3 e{c == 3 ? 1.f : 0.f, c == 4 ? 1.f : 0.f, c == 5 ? 1.f : 0.f};
+            om = qrot(B.w, B.i, B.j, B.k, e);
+            v = cross(V3{B.x, B.y, B.z}, om);
+        }
+        return;
+    }
+    const int a = c - boff;
+    v = V3{0.f, 0.f, 0.f};
+    om = V3{0.f, 0.f, 0.f};
+    const unsigned long long anc = t.lanc[link];
+    for (int idx = t.colstart[a]; idx < t.colstart[a + 1]; ++idx) {
+        const int j = t.coljoint[idx];
+        if ((anc >> j) & 1ull) {
+            const float m = t.colmul[idx];
+            const float* s = S + 8 * j;
+            v = v + m * V3{s[0], s[1], s[2]};
+            om = om + m * V3{s[3], s[4], s[5]};
+        }
+    }
+}
+
+// d(distance between sphere centres ci, cj)/d(column c), scaled
+// (self_collision_task.py:260-321)
+__device__ __forceinline__ float collision_column(const Tabs& t, const float* S, const float* base, int c, int li,
+                                                  int lj, V3 ci, V3 cj, V3 n) {
+    const int boff = t.h->base_off;
+    if (c < boff) {
+        if (c < 3) return 0.f;
+        const Pose B = pose_load(base);
+        const V3 e{c == 3 ? 1.f : 0.f, c == 4 ? 1.f : 0.f, c == 5 ? 1.f : 0.f};
+        const V3 om = qrot(B.w, B.i, B.j, B.k, e);
+        return dot(n, cross(om, ci - cj));
+    }
+    const int a = c - boff;
+    const unsigned long long ai = t.lanc[li], aj = t.lanc[lj];
+    float val = 0.f;
+    for (int idx = t.colstart[a]; idx < t.colstart[a + 1]; ++idx) {
+        const int j = t.coljoint[idx];
+        const bool bi = (ai >> j) & 1ull, bj = (aj >> j) & 1ull;
+        if (!bi && !bj) continue;
+        const float* s = S + 8 * j;
+        const V3 v{s[0], s[1], s[2]}, om{s[3], s[4], s[5]};
+        V3 col_i{0.f, 0.f, 0.f}, col_j{0.f, 0.f, 0.f};
+        if (bi) col_i = v + cross(om, ci);
+        if (bj) col_j = v + cross(om, cj);
+        val += t.colmul[idx] * dot(n, col_i - col_j);
+    }
+    return val;
+}
+
+// ---------------------------------------------------------------------------
+// evaluation of every residual at one point (the cost pass of _accept_body,
+// lm_optimizer.py:964-982): FK, spheres, pose/limit/collision residuals,
+// cost = 0.5 |r|^2 and the pose errors of the metrics kernel (helpers/ik/ik.py:60-82).
+// ---------------------------------------------------------------------------
+struct EvalOut {
+    float cost;
+    float max_pos;  // largest position error over position entries [m]
+    float max_rot;  // largest angle error over rotation entries [rad]
+    float* Tj;      // FK buffer holding T_world_joint
+    float* S;       // the other FK buffer
+    int nslots;     // filled slots summed over slot-mode terms
+};
+
+template <int G>
+__device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
+    const TabHeader* h = t.h;
+    EvalOut o;
+    o.Tj = group_fk<G>(g, t, w, q, base);
+    o.S = (o.Tj == w.T0) ? w.T1 : w.T0;
+    float* Tj = o.Tj;
+    const bool need_sph = h->ncoll > 0;
+    if (need_sph) {
+        for (int s = g.lane; s < h->ns; s += G) {
+            const Pose P = link_pose(t, Tj, base, t.sphlink[s]);
+            const float* c = t.sph + 4 * s;
+            const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
+            *reinterpret_cast<float4*>(w.sph + 4 * s) = make_float4(wc.x, wc.y, wc.z, c[3]);
+        }
+        if (h->max_slots > 0) {
+            for (int l = g.lane; l < h->nl; l += G) {
+                const Pose P = link_pose(t, Tj, base, l);
+                const float* c = t.lbound + 4 * l;
+                const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
+                *reinterpret_cast<float4*>(w.lbw + 4 * l) = make_float4(wc.x, wc.y, wc.z, c[3]);
+            }
+        }
+        g.sync();
+    }
+    float ks = 0.f, kc = 0.f;
+    float max_pos = 0.f, max_rot = 0.f;
+    // pose entries
+    for (int e = g.lane; e < h->npose; e += G) {
+        const PoseEntry& pe = t.pose[e];
+        const Pose P = link_pose(t, Tj, base, pe.link);
+        const float* tg = w.tgt + 8 * e;
+        V3 r;
+        if (pe.kind == kPosePosition) {
+            const V3 err{tg[0] - P.x, tg[1] - P.y, tg[2] - P.z};
+            max_pos = fmaxf(max_pos, norm3(err));
+            r = V3{pe.w[0] * err.x, pe.w[1] * err.y, pe.w[2] * err.z};
+        } else {
+            float qw, qi, qj, qk;
+            qmul_std(P.w, P.i, P.j, P.k, tg[3], -tg[4], -tg[5], -tg[6], qw, qi, qj, qk);
+            const V3 aa = quat_to_axis_angle(qw, qi, qj, qk);
+            const float sn = fminf(sqrtf(qi * qi + qj * qj + qk * qk), 1.0f);
+            max_rot = fmaxf(max_rot, 2.0f * asinf(sn));
+            r = V3{pe.w[0] * aa.x, pe.w[1] * aa.y, pe.w[2] * aa.z};
+        }
+        w.rpose[3 * e] = r.x;
+        w.rpose[3 * e + 1] = r.y;
+        w.rpose[3 * e + 2] = r.z;
+        kadd(ks, kc, r.x * r.x);
+        kadd(ks, kc, r.y * r.y);
+        kadd(ks, kc, r.z * r.z);
+    }
+    // joint limits, position_limit.py:509-534 ("abs")
+    if (h->has_limit) {
+        for (int a = g.lane; a < h->na; a += G) {
+            const float v = q[a];
+            const float lo = t.lim[2 * a], hi = t.lim[2 * a + 1];
+            const float err = fmaxf(0.f, v - hi) + fmaxf(0.f, lo - v);
+            const float r = t.limw[a] * err;
+            w.rlim[a] = r;
+            kadd(ks, kc, r * r);
+        }
+    }
+    // self collision, self_collision_task.py:73-256
+    o.nslots = 0;
+    for (int ci = 0; ci < h->ncoll; ++ci) {
+        const CollEntry& ce = t.coll[ci];
+        const int* spk = t.at<int>(ce.o_sp);
+        if (ce.mode == 1) {
+            for (int p = g.lane; p < ce.nsp; p += G) {
+                const int pk = spk[p];
+                const int si = pk & 0xffff, sj = pk >> 16;
+                const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * si);
+                const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * sj);
+                const float d = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z});
+                const float pen = ce.margin - (d - a.w - b.w);
+                if (pen > 0.f) {
+                    const float r = ce.weight * pen;
+                    kadd(ks, kc, r * r);
+                }
+            }
+        } else {
+            const int* lp = t.at<int>(ce.o_lp);
+            const int* lpoff = t.at<int>(ce.o_lpoff);
+            Slot* slots = reinterpret_cast<Slot*>(w.raw + ce.ws_slots);
+            int count = 0;
+            // broad phase in link-pair order; the first K penetrating link pairs take the slots
+            for (int b0 = 0; b0 < ce.nlp; b0 += G) {
+                const int l = b0 + g.lane;
+                bool act = false;
+                if (l < ce.nlp) {
+                    const float4 a = *reinterpret_cast<const float4*>(w.lbw + 4 * lp[2 * l]);
+                    const float4 b = *reinterpret_cast<const float4*>(w.lbw + 4 * lp[2 * l + 1]);
+                    const float d = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z});
+                    act = (a.w + b.w + ce.margin - d) > 0.f;
+                }
+                const unsigned bal = g.ballot(act);
+                const int pos = count + __popc(bal & g.lt_mask());
+                if (act && pos < ce.K) slots[pos].lp = l;
+                count += __popc(bal);
+            }
+            const int nsl = min(count, ce.K);
+            g.sync();
+            // narrow phase: first strict minimum of the surface distance per kept link pair
+            for (int k = g.lane; k < nsl; k += G) {
+                const int l = slots[k].lp;
+                float best = 1.0e10f;
+                int bp = lpoff[l];
+                for (int p = lpoff[l]; p < lpoff[l + 1]; ++p) {
+                    const int pk = spk[p];
+                    const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * (pk & 0xffff));
+                    const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * (pk >> 16));
+                    const float s = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z}) - a.w - b.w;
+                    if (s < best) {
+                        best = s;
+                        bp = p;
+                    }
+                }
+                const int pk = spk[bp];
+                const int si = pk & 0xffff, sj = pk >> 16;
+                const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * si);
+                const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * sj);
+                const float surf = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z}) - a.w - b.w;
+                const float r = ce.weight * fmaxf(0.f, ce.margin - surf);
+                slots[k].i = si;
+                slots[k].j = sj;
+                slots[k].r = r;
+                kadd(ks, kc, r * r);
+            }
+            reinterpret_cast<int*>(w.misc)[8 + ci] = nsl;
+            o.nslots += nsl;
+        }
+    }
+    o.cost = 0.5f * group_ksum<G>(g, ks, kc);
+    o.max_pos = g.maxf(max_pos);
+    o.max_rot = g.maxf(max_rot);
+    g.sync();
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// linearisation at the last evaluated point: motion subspace, Jacobian rows in
+// chunks, compensated J^T J / J^T r accumulation, joint-limit diagonal and the
+// active-DOF mask (lm_optimizer.py:145-189, 872-880; position_task.py:216-272;
+// rotation_task.py:353-401; position_limit.py:538-573;
+// self_collision_task.py:325-385).  Result: w.Hs[0:T] packed lower J^T J,
+// w.Hs[T:T+D] J^T r.
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ void group_accumulate_chunk(const Group<G>& g, const Tabs& t, Ws& w, int nrows) {
+    const TabHeader* h = t.h;
+    const int Dp = h->Dp, T = h->T, E = h->E;
+    for (int e = g.lane; e < E; e += G) {
+        float s = 0.f;
+        if (e < T) {
+            const unsigned ab = t.ab[e];
+            const int a = ab >> 8, b = ab & 0xff;
+            const float* ja = w.Jc + a;
+            const float* jb = w.Jc + b;
+            for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], jb[r * Dp], s);
+        } else {
+            const float* ja = w.Jc + (e - T);
+            for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], w.rc[r], s);
+        }
+        float hs = w.Hs[e], hc = w.Hc[e];
+        kadd(hs, hc, s);
+        w.Hs[e] = hs;
+        w.Hc[e] = hc;
+    }
+    g.sync();
+}
+
+// Build the Jacobian of pose entries [e0, e0+ne) into the chunk (3 rows each).
+template <int G>
+__device__ void group_pose_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* Tj, const float* S,
+                                const float* base, int e0, int ne) {
+    const int D = t.h->D, Dp = t.h->Dp;
+    const int items = ne * D;
+    for (int it = g.lane; it < items; it += G) {
+        const int el = it / D, c = it - el * D;
+        const PoseEntry& pe = t.pose[e0 + el];
+        V3 v, om;
+        column_twist(t, S, base, c, pe.link, v, om);
+        float* J = w.Jc + (3 * el) * Dp + c;
+        if (pe.kind == kPosePosition) {
+            const Pose P = link_pose(t, Tj, base, pe.link);
+            const V3 pv = v + cross(om, V3{P.x, P.y, P.z});
+            J[0] = -pe.w[0] * pv.x;
+            J[Dp] = -pe.w[1] * pv.y;
+            J[2 * Dp] = -pe.w[2] * pv.z;
+        } else {
+            J[0] = pe.w[0] * om.x;
+            J[Dp] = pe.w[1] * om.y;
+            J[2 * Dp] = pe.w[2] * om.z;
+        }
+    }
+    for (int r = g.lane; r < 3 * ne; r += G) w.rc[r] = w.rpose[3 * e0 + r];
+    g.sync();
+}
+
+// Build collision rows from rowmeta (i, j, residual) records into the chunk.
+template <int G>
+__device__ void group_collision_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* S, const float* base,
+                                     const CollEntry& ce, int nrows) {
+    const int D = t.h->D, Dp = t.h->Dp;
+    const int items = nrows * D;
+    for (int it = g.lane; it < items; it += G) {
+        const int r = it / D, c = it - r * D;
+        const float* m = w.rowmeta + 8 * r;
+        const int si = __float_as_int(m[0]), sj = __float_as_int(m[1]);
+        const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * si);
+        const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * sj);
+        const V3 ci{a.x, a.y, a.z}, cj{b.x, b.y, b.z};
+        const V3 diff = ci - cj;
+        const float dist = norm3(diff);
+        const float surf = dist - a.w - b.w;
+        const float pen = ce.margin - surf;
+        float val = 0.f;
+        if (pen > 0.f) {
+            const float den = fmaxf(1e-8f, dist);
+            const V3 n{diff.x / den, diff.y / den, diff.z / den};
+            val = -ce.weight * collision_column(t, S, base, c, t.sphlink[si], t.sphlink[sj], ci, cj, n);
+        }
+        w.Jc[r * Dp + c] = val;
+    }
+    for (int r = g.lane; r < nrows; r += G) w.rc[r] = w.rowmeta[8 * r + 2];
+    g.sync();
+}
+
+template <int G>
+__device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const EvalOut& ev, const float* base) {
+    const TabHeader* h = t.h;
+    const int D = h->D, T = h->T, E = h->E;
+    float* S = ev.S;
+    const float* Tj = ev.Tj;
+    for (int j = g.lane; j < h->nj; j += G) {
+        V3 v, om;
+        joint_subspace(t, Tj, j, v, om);
+        float* s = S + 8 * j;
+        s[0] = v.x;
+        s[1] = v.y;
+        s[2] = v.z;
+        s[3] = om.x;
+        s[4] = om.y;
+        s[5] = om.z;
+    }
+    for (int e = g.lane; e < E; e += G) {
+        w.Hs[e] = 0.f;
+        w.Hc[e] = 0.f;
+    }
+    g.sync();
+    // pose rows, kChunkRows/3 entries per chunk
+    constexpr int PE = kChunkRows / 3;
+    for (int e0 = 0; e0 < h->npose; e0 += PE) {
+        const int ne = min(PE, h->npose - e0);
+        group_pose_rows<G>(g, t, w, Tj, S, base, e0, ne);
+        group_accumulate_chunk<G>(g, t, w, 3 * ne);
+    }
+    // collision rows
+    for (int ci = 0; ci < h->ncoll; ++ci) {
+        const CollEntry& ce = t.coll[ci];
+        if (ce.mode == 0) {
+            const Slot* slots = reinterpret_cast<const Slot*>(w.raw + ce.ws_slots);
+            const int nsl = reinterpret_cast<const int*>(w.misc)[8 + ci];
+            for (int k0 = 0; k0 < nsl; k0 += kChunkRows) {
+                const int nr = min(kChunkRows, nsl - k0);
+                for (int r = g.lane; r < nr; r += G) {
+                    float* m = w.rowmeta + 8 * r;
+                    m[0] = __int_as_float(slots[k0 + r].i);
+                    m[1] = __int_as_float(slots[k0 + r].j);
+                    m[2] = slots[k0 + r].r;
+                }
+                g.sync();
+                group_collision_rows<G>(g, t, w, S, base, ce, nr);
+                group_accumulate_chunk<G>(g, t, w, nr);
+            }
+        } else {
+            const int* spk = t.at<int>(ce.o_sp);
+            int filled = 0;
+            for (int b0 = 0; b0 < ce.nsp; b0 += G) {
+                const int p = b0 + g.lane;
+                bool act = false;
+                float r = 0.f;
+                int pk = 0;
+                if (p < ce.nsp) {
+                    pk = spk[p];
+                    const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * (pk & 0xffff));
+                    const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * (pk >> 16));
+                    const float d = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z});
+                    const float pen = ce.margin - (d - a.w - b.w);
+                    act = pen > 0.f;
+                    r = ce.weight * pen;
+                }
+                const unsigned bal = g.ballot(act);
+                if (act) {
+                    float* m = w.rowmeta + 8 * (filled + __popc(bal & g.lt_mask()));
+                    m[0] = __int_as_float(pk & 0xffff);
+                    m[1] = __int_as_float(pk >> 16);
+                    m[2] = r;
+                }
+                filled += __popc(bal);
+                const bool last = b0 + G >= ce.nsp;
+                if (filled > kChunkRows - G || (last && filled > 0)) {
+                    g.sync();
+                    group_collision_rows<G>(g, t, w, S, base, ce, filled);
+                    group_accumulate_chunk<G>(g, t, w, filled);
+                    filled = 0;
+                }
+            }
+        }
+    }
+    // finalise: fold compensation, joint-limit diagonal, active-DOF mask
+    const int boff = h->base_off;
+    for (int e = g.lane; e < E; e += G) {
+        float v = w.Hs[e] + w.Hc[e];
+        int a, b;
+        if (e < T) {
+            const unsigned ab = t.ab[e];
+            a = ab >> 8;
+            b = ab & 0xff;
+            if (h->has_limit && a == b && a >= boff) {
+                const int k = a - boff;
+                const float qv = w.q[k];
+                const float lo = t.lim[2 * k], hi = t.lim[2 * k + 1];
+                const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
+                const float js = t.limw[k] * sg;
+                v += js * js;
+            }
+        } else {
+            a = e - T;
+            b = a;
+            if (h->has_limit && a >= boff) {
+                const int k = a - boff;
+                const float qv = w.q[k];
+                const float lo = t.lim[2 * k], hi = t.lim[2 * k + 1];
+                const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
+                v += t.limw[k] * sg * w.rlim[k];
+            }
+        }
+        if (h->mask_any) v *= (e < T) ? t.mask[a] * t.mask[b] : t.mask[a];
+        w.Hs[e] = v;
+    }
+    g.sync();
+}
+
+// ---------------------------------------------------------------------------
+// damped FP64 Cholesky solve (lm_optimizer.py:56-79 / 145-189):
+//   (H + lambda I) delta = -g,  pred = 0.5 delta . (lambda delta - g)
+// H packed lower in `Hp` (fp32), g in Hp[T:].  Step in w.y (fp64) and w.d32.
+// Returns false when a pivot is not positive (delta = 0, pred = 0).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int tri(int i, int j) { return (i * (i + 1)) / 2 + j; }
+
+template <int G>
+__device__ bool group_damped_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
+                                   double& pred, double& dnorm) {
+    const int D = t.h->D, T = t.h->T;
+    double* L = w.L;
+    const double lam = (double)lambda_f;
+    for (int e = g.lane; e < T; e += G) {
+        const unsigned ab = t.ab[e];
+        double v = (double)Hp[e];
+        if ((ab >> 8) == (ab & 0xff)) v += lam;
+        L[e] = v;
+    }
+    for (int i = g.lane; i < D; i += G) w.y[i] = -(double)Hp[T + i];
+    g.sync();
+    bool ok = true;
+    for (int k = 0; k < D; ++k) {
+        const double akk = L[tri(k, k)];
+        if (!(akk > 0.0)) {
+            ok = false;
+            break;
+        }
+        const double d = sqrt(akk);
+        const double inv = 1.0 / d;
+        g.sync();
+        for (int i = k + 1 + g.lane; i < D; i += G) {
+            const double l = L[tri(i, k)] * inv;
+            L[tri(i, k)] = l;
+            w.tmp[i] = l;
+        }
+        if (g.lane == 0) L[tri(k, k)] = d;
+        g.sync();
+        // trailing update over the (i, j) items k < j <= i, strided by lane
+        const int m = D - k - 1;
+        int i = k + 1, jj = k + 1 + g.lane;  // row i, column jj
+        while (i < D && jj > i) {
+            jj -= (i - k);
+            ++i;
+        }
+        while (i < D) {
+            L[tri(i, jj)] -= w.tmp[i] * w.tmp[jj];
+            jj += G;
+            while (i < D && jj > i) {
+                jj -= (i - k);
+                ++i;
+            }
+        }
+        (void)m;
+        g.sync();
+    }
+    if (!ok) {
+        g.sync();
+        for (int i = g.lane; i < D; i += G) {
+            w.y[i] = 0.0;
+            w.d32[i] = 0.f;
+        }
+        pred = 0.0;
+        dnorm = 0.0;
+        g.sync();
+        return false;
+    }
+    // forward substitution L z = -g
+    for (int k = 0; k < D; ++k) {
+        const double zk = w.y[k] / L[tri(k, k)];
+        g.sync();
+        if (g.lane == 0) w.y[k] = zk;
+        for (int i = k + 1 + g.lane; i < D; i += G) w.y[i] -= L[tri(i, k)] * zk;
+        g.sync();
+    }
+    // back substitution L^T x = z
+    for (int k = D - 1; k >= 0; --k) {
+        const double xk = w.y[k] / L[tri(k, k)];
+        g.sync();
+        if (g.lane == 0) w.y[k] = xk;
+        for (int i = g.lane; i < k; i += G) w.y[i] -= L[tri(k, i)] * xk;
+        g.sync();
+    }
+    double pp = 0.0, nn = 0.0;
+    for (int i = g.lane; i < D; i += G) {
+        const double x = w.y[i];
+        const double gi = (double)Hp[T + i];
+        pp += x * (lam * x - gi);
+        nn += x * x;
+        w.d32[i] = (float)x;
+    }
+    pred = 0.5 * g.sumd(pp);
+    dnorm = sqrt(g.sumd(nn));
+    g.sync();
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// integrate, robo/robot_kernels.py:563-644 (q + mask * delta; base * exp(delta_base))
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ void group_integrate(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base, float* qo,
+                                float* baseo) {
+    const TabHeader* h = t.h;
+    const int boff = h->base_off;
+    for (int a = g.lane; a < h->na; a += G) {
+        const float m = h->mask_any ? t.mask[boff + a] : 1.f;
+        qo[a] = q[a] + m * w.d32[boff + a];
+    }
+    if (boff && g.lane == 0) {
+        float xi[6];
+        for (int k = 0; k < 6; ++k) xi[k] = w.d32[k];
+        if (h->mask_any)
+            for (int k = 3; k < 6; ++k) xi[k] *= t.mask[k];
+        const Pose B = pose_load(base);
+        Pose N = compose(B, se3_exp(xi, 1e-4f));
+        if (h->mask_any) {
+            if (t.mask[0] == 0.f) N.x = B.x;
+            if (t.mask[1] == 0.f) N.y = B.y;
+            if (t.mask[2] == 0.f) N.z = B.z;
+        }
+        pose_store(baseo, N);
+    }
+    g.sync();
+}
+
+}  // namespace b200ik

@@ -1,0 +1,785 @@
+// ik_kernels.cuh — solver and single-stage kernels built from ik_device.cuh.
+#pragma once
+#include "b200ik.h"
+#include "ik_device.cuh"
+
+namespace b200ik {
+
+constexpr int kBlockThreads = 128;
+
+// Per-problem record the plain form keeps in HBM between its per-iteration
+// launches: cached normal equations of the current point plus scalars.
+struct RecScalars {
+    float cost, lambda, pos_err, rot_err;
+    int status, iters, pad0, pad1;
+};
+__host__ __device__ inline int rec_stride(int E) { return ((E + 8) + 3) & ~3; }
+
+// per-problem solver state kept in registers (identical in every lane of the group)
+struct LmState {
+    float cost, lambda, pos_err, rot_err;
+    int status, iters;
+};
+
+// Stage the table blob into shared memory; returns the start of group workspaces.
+__device__ __forceinline__ char* stage_tables(const char* __restrict__ blob, char* smem) {
+    const TabHeader* gh = reinterpret_cast<const TabHeader*>(blob);
+    const int n16 = gh->bytes >> 4;
+    const int4* src = reinterpret_cast<const int4*>(blob);
+    int4* dst = reinterpret_cast<int4*>(smem);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    return smem + gh->bytes;
+}
+
+template <int G>
+__device__ __forceinline__ void load_point(const Group<G>& g, const Tabs& t, Ws& w, int p, const float* q,
+                                           const float* base) {
+    const TabHeader* h = t.h;
+    for (int a = g.lane; a < h->na; a += G) w.q[a] = q[(size_t)p * h->na + a];
+    if (h->base_off && g.lane < 7) w.base[g.lane] = base[(size_t)p * 7 + g.lane];
+}
+
+template <int G>
+__device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
+    const TabHeader* h = t.h;
+    const int items = h->npose * 7;
+    for (int it = g.lane; it < items; it += G) {
+        const int e = it / 7, c = it - 7 * e;
+        const PoseEntry& pe = t.pose[e];
+        const int rows = pe.target_rows > 0 ? pe.target_rows : batch;
+        int rep = batch / rows;
+        if (rep < 1) rep = 1;
+        const int row = min(p / rep, rows - 1);
+        w.tgt[8 * e + c] = pe.targets[((size_t)row * pe.num_frames + pe.frame) * 7 + c];
+    }
+}
+
+template <int G>
+__device__ __forceinline__ const float* cur_base(const Tabs& t, const Ws& w) {
+    return t.h->base_off ? w.base : nullptr;
+}
+
+template <int G>
+__device__ __forceinline__ bool check_stop(LmState& st, const IkLmParams& P) {
+    bool stop = false;
+    if ((P.stop_rules & IK_STOP_POSE) && st.pos_err <= P.pose_pos_tol && st.rot_err <= P.pose_rot_tol) stop = true;
+    if ((P.stop_rules & IK_STOP_COST) && st.cost <= P.cost_tol) stop = true;
+    if (stop) st.status |= IK_ST_CONVERGED;
+    return stop;
+}
+
+// Start a solve at the loaded point: evaluate, linearise, set damping.
+template <int G>
+__device__ void group_start(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P) {
+    const EvalOut ev = group_eval<G>(g, t, w, w.q, cur_base<G>(t, w));
+    st.cost = ev.cost;
+    st.pos_err = ev.max_pos;
+    st.rot_err = ev.max_rot;
+    st.lambda = P.lambda_init;
+    st.status = isfinite(ev.cost) ? IK_ST_RUNNING : IK_ST_NONFINITE;
+    st.iters = 0;
+    group_linearize<G>(g, t, w, ev, cur_base<G>(t, w));
+}
+
+struct StepTrace {  // optional per-step outputs (ik_step)
+    float cost_before, cost_new, pred;
+    int accepted;
+};
+
+// One LM iteration from the cached linearisation (LMOptimizer._step_body,
+// lm_optimizer.py:834-1005).  Returns true when the problem stops.
+template <int G>
+__device__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
+                              StepTrace* trace = nullptr) {
+    double pred = 0.0, dnorm = 0.0;
+    const bool ok = group_damped_solve<G>(g, t, w, w.Hs, st.lambda, pred, dnorm);
+    if (!ok) st.status |= IK_ST_NOT_SPD;
+    if ((P.stop_rules & IK_STOP_STEP) && ok && dnorm < (double)P.step_tol && trace == nullptr) {
+        st.status |= IK_ST_CONVERGED;
+        return true;
+    }
+    const bool floating = t.h->base_off != 0;
+    group_integrate<G>(g, t, w, w.q, w.base, w.qp, w.basep);
+    const EvalOut ev = group_eval<G>(g, t, w, w.qp, floating ? w.basep : nullptr);
+    // gain ratio in FP64 (lm_optimizer.py:319-329)
+    bool acc = pred > 0.0;
+    if (acc) {
+        const double rho = ((double)st.cost - (double)ev.cost) / (pred + (double)P.gain_ratio_epsilon);
+        acc = rho >= (double)P.rho_min;
+    }
+    if (trace) {
+        trace->cost_before = st.cost;
+        trace->cost_new = ev.cost;
+        trace->pred = (float)pred;
+        trace->accepted = acc ? 1 : 0;
+    }
+    if (acc) {
+        float* tq = w.q;
+        w.q = w.qp;
+        w.qp = tq;
+        float* tb = w.base;
+        w.base = w.basep;
+        w.basep = tb;
+        st.cost = ev.cost;
+        st.pos_err = ev.max_pos;
+        st.rot_err = ev.max_rot;
+        st.lambda = fmaxf(st.lambda / P.lambda_factor, P.lambda_min);
+        group_linearize<G>(g, t, w, ev, floating ? w.base : nullptr);
+    } else {
+        st.lambda = fminf(fmaxf(st.lambda * P.lambda_factor, P.lambda_min), P.lambda_max);
+    }
+    st.iters += 1;
+    bool stop = check_stop<G>(st, P);
+    if (!stop && st.iters >= P.max_iter) {
+        st.status |= IK_ST_MAX_ITER;
+        stop = true;
+    }
+    return stop;
+}
+
+template <int G>
+__device__ void store_solution(const Group<G>& g, const Tabs& t, const Ws& w, const LmState& st, int p, float* q,
+                               float* base, float* cost, float* lambda, int* iters, int* status) {
+    const TabHeader* h = t.h;
+    for (int a = g.lane; a < h->na; a += G) q[(size_t)p * h->na + a] = w.q[a];
+    if (h->base_off && g.lane < 7) base[(size_t)p * 7 + g.lane] = w.base[g.lane];
+    if (g.lane == 0) {
+        if (cost) cost[p] = st.cost;
+        if (lambda) lambda[p] = st.lambda;
+        if (iters) iters[p] = st.iters;
+        if (status) status[p] = st.status;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// plain form: mode 0 = start (evaluate + linearise), mode 1 = one iteration.
+// Static grid-stride over problems; state round-trips through `rec`.
+// counters[0..2]: per-iteration "cost above tolerance" counts, counters[3]:
+// sticky stop flag of the all-problems cost rule (opt/optimizer.py:237-239).
+// ---------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __restrict__ blob, int batch, float* q,
+                                                                float* base, float* rec, IkLmParams P, int mode,
+                                                                int k, int* counters, float* out_cost,
+                                                                float* out_lambda, int* out_iters, int* out_status) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    const bool all_rule = (P.stop_rules & IK_STOP_ALL_COST) != 0;
+    if (mode == 1 && all_rule) {
+        if (counters[3] != 0) return;
+        const int interval = P.check_interval > 0 ? P.check_interval : 1;
+        if (k >= 1 && (k % interval) == 0 && counters[(k - 1) % 3] == 0) {
+            if (threadIdx.x == 0) counters[3] = 1;
+            return;
+        }
+    }
+    if (mode == 0 && blockIdx.x == 0 && threadIdx.x < 4) counters[threadIdx.x] = 0;
+    if (mode == 1 && blockIdx.x == 0 && threadIdx.x == 0) counters[(k + 1) % 3] = 0;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int rs = rec_stride(h->E);
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        float* r = rec + (size_t)p * rs;
+        RecScalars* rsc = reinterpret_cast<RecScalars*>(r + h->E);
+        LmState st;
+        bool touched = true;
+        load_point<G>(g, t, w, p, q, base);
+        load_targets<G>(g, t, w, p, batch);
+        if (mode == 0) {
+            g.sync();
+            group_start<G>(g, t, w, st, P);
+            check_stop<G>(st, P);
+            if (P.max_iter <= 0) st.status |= IK_ST_MAX_ITER;
+        } else {
+            const RecScalars s = *rsc;
+            st.cost = s.cost;
+            st.lambda = s.lambda;
+            st.pos_err = s.pos_err;
+            st.rot_err = s.rot_err;
+            st.status = s.status;
+            st.iters = s.iters;
+            const bool done = (st.status & (IK_ST_CONVERGED | IK_ST_MAX_ITER | IK_ST_NONFINITE)) != 0;
+            touched = !done;
+            if (!done) {
+                for (int e = g.lane; e < h->E; e += G) w.Hs[e] = r[e];
+                g.sync();
+                group_iterate<G>(g, t, w, st, P);
+                // the all-problems rule decides the iteration count; without it the cap is max_iter
+            }
+        }
+        if (all_rule && g.lane == 0 && mode == 1 && !(st.cost <= P.cost_tol)) atomicAdd(&counters[k % 3], 1);
+        g.sync();
+        if (touched)
+            for (int e = g.lane; e < h->E; e += G) r[e] = w.Hs[e];
+        if (g.lane == 0) {
+            RecScalars s;
+            s.cost = st.cost;
+            s.lambda = st.lambda;
+            s.pos_err = st.pos_err;
+            s.rot_err = st.rot_err;
+            s.status = st.status;
+            s.iters = st.iters;
+            s.pad0 = s.pad1 = 0;
+            *rsc = s;
+        }
+        store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
+        g.sync();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// persistent form: groups pull problems from a device work queue and iterate
+// each to its own stop rule inside the launch.
+// ---------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) lm_persistent_kernel(const char* __restrict__ blob, int batch,
+                                                                     float* q, float* base, IkLmParams P,
+                                                                     int* queue, float* out_cost, float* out_lambda,
+                                                                     int* out_iters, int* out_status) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    while (true) {
+        int p = 0;
+        if (g.lane == 0) p = atomicAdd(queue, 1);
+        p = g.bcast(p, 0);
+        if (p >= batch) break;
+        load_point<G>(g, t, w, p, q, base);
+        load_targets<G>(g, t, w, p, batch);
+        g.sync();
+        LmState st;
+        group_start<G>(g, t, w, st, P);
+        bool stop = (st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0;
+        while (!stop) stop = group_iterate<G>(g, t, w, st, P);
+        if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
+        store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
+        g.sync();
+        // restore the canonical buffer order (the accept path swaps q/qp and base/basep)
+        w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// single-stage kernels
+// ---------------------------------------------------------------------------
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) fk_kernel(const char* __restrict__ blob, int batch, const float* q,
+                                                          const float* base, float* T_joint, float* T_link,
+                                                          float* S_world, float* spheres, float* link_bounds) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int nj = h->nj, nl = h->nl, ns = h->ns;
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        load_point<G>(g, t, w, p, q, base);
+        g.sync();
+        const float* b = cur_base<G>(t, w);
+        float* Tj = group_fk<G>(g, t, w, w.q, b);
+        if (T_joint)
+            for (int it = g.lane; it < nj * 7; it += G) {
+                const int j = it / 7, c = it - 7 * j;
+                T_joint[((size_t)p * nj + j) * 7 + c] = Tj[8 * j + c];
+            }
+        if (T_link)
+            for (int it = g.lane; it < nl * 7; it += G) {
+                const int l = it / 7, c = it - 7 * l;
+                const int j = t.lpj[l];
+                float v;
+                if (j >= 0)
+                    v = Tj[8 * j + c];
+                else
+                    v = b ? b[c] : (c == 3 ? 1.f : 0.f);
+                T_link[((size_t)p * nl + l) * 7 + c] = v;
+            }
+        if (S_world)
+            for (int j = g.lane; j < nj; j += G) {
+                V3 v, om;
+                joint_subspace(t, Tj, j, v, om);
+                float* s = S_world + (size_t)p * 6 * nj;
+                s[0 * nj + j] = v.x;
+                s[1 * nj + j] = v.y;
+                s[2 * nj + j] = v.z;
+                s[3 * nj + j] = om.x;
+                s[4 * nj + j] = om.y;
+                s[5 * nj + j] = om.z;
+            }
+        if (spheres)
+            for (int s = g.lane; s < ns; s += G) {
+                const Pose P = link_pose(t, Tj, b, t.sphlink[s]);
+                const float* c = t.sph + 4 * s;
+                const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
+                float* o = spheres + ((size_t)p * ns + s) * 3;
+                o[0] = wc.x;
+                o[1] = wc.y;
+                o[2] = wc.z;
+            }
+        if (link_bounds)
+            for (int l = g.lane; l < nl; l += G) {
+                const Pose P = link_pose(t, Tj, b, l);
+                const float* c = t.lbound + 4 * l;
+                const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
+                float* o = link_bounds + ((size_t)p * nl + l) * 3;
+                o[0] = wc.x;
+                o[1] = wc.y;
+                o[2] = wc.z;
+            }
+        g.sync();
+    }
+}
+
+// link Jacobian, robo/robot_kernels.py:668-737 (frame 0 spatial, 1 body)
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) link_jacobian_kernel(const char* __restrict__ blob, int batch,
+                                                                     const float* q, const float* base, int link,
+                                                                     int body, float* J) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int D = h->D, boff = h->base_off;
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        load_point<G>(g, t, w, p, q, base);
+        g.sync();
+        const float* b = cur_base<G>(t, w);
+        float* Tj = group_fk<G>(g, t, w, w.q, b);
+        float* S = (Tj == w.T0) ? w.T1 : w.T0;
+        for (int j = g.lane; j < h->nj; j += G) {
+            V3 v, om;
+            joint_subspace(t, Tj, j, v, om);
+            float* s = S + 8 * j;
+            s[0] = v.x;
+            s[1] = v.y;
+            s[2] = v.z;
+            s[3] = om.x;
+            s[4] = om.y;
+            s[5] = om.z;
+        }
+        g.sync();
+        const Pose F = link_pose(t, Tj, b, link);
+        for (int c = g.lane; c < D; c += G) {
+            V3 v, om;
+            if (c < boff) {
+                const Pose B = pose_load(b);
+                if (body) {
+                    // Ad(T_frame_base) e_c with T_frame_base = T_frame_world o T_world_base
+                    const Pose Fi{0.f, 0.f, 0.f, F.w, -F.i, -F.j, -F.k};
+                    const V3 ti = qrot(Fi.w, Fi.i, Fi.j, Fi.k, V3{F.x, F.y, F.z});
+                    const Pose Finv{-ti.x, -ti.y, -ti.z, F.w, -F.i, -F.j, -F.k};
+                    const Pose FB = compose(Finv, B);
+                    if (c < 3) {
+                        const V3 e{c == 0 ? 1.f : 0.f, c == 1 ? 1.f : 0.f, c == 2 ? 1.f : 0.f};
+                        v = qrot(FB.w, FB.i, FB.j, FB.k, e);
+                        om = V3{0.f, 0.f, 0.f};
+                    } else {
+                        const V3 e{c == 3 ? 1.f : 0.f, c == 4 ? 1.f : 0.f, c == 5 ? 1.f : 0.f};
+                        om = qrot(FB.w, FB.i, FB.j, FB.k, e);
+                        v = cross(V3{FB.x, FB.y, FB.z}, om);
+                    }
+                } else {
+                    column_twist(t, S, b, c, link, v, om);
+                }
+            } else {
+                column_twist(t, S, b, c, link, v, om);
+                if (body) {
+                    // Ad(T_frame_world) [v; w] = [R^T (v - t x w); R^T w]
+                    const V3 tf{F.x, F.y, F.z};
+                    const V3 vv = v - cross(tf, om);
+                    v = qrot(F.w, -F.i, -F.j, -F.k, vv);
+                    om = qrot(F.w, -F.i, -F.j, -F.k, om);
+                }
+            }
+            float* o = J + (size_t)p * 6 * D;
+            o[0 * D + c] = v.x;
+            o[1 * D + c] = v.y;
+            o[2 * D + c] = v.z;
+            o[3 * D + c] = om.x;
+            o[4 * D + c] = om.y;
+            o[5 * D + c] = om.z;
+        }
+        g.sync();
+    }
+}
+
+// residuals + Jacobian rows in the reference row layout (outputs pre-zeroed)
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __restrict__ blob, int batch,
+                                                              const float* q, const float* base, float* rout,
+                                                              float* Jout) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int D = h->D, Dp = h->Dp, R = h->R_ref, boff = h->base_off;
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        load_point<G>(g, t, w, p, q, base);
+        load_targets<G>(g, t, w, p, batch);
+        g.sync();
+        const float* b = cur_base<G>(t, w);
+        const EvalOut ev = group_eval<G>(g, t, w, w.q, b);
+        float* ro = rout ? rout + (size_t)p * R : nullptr;
+        float* Jo = Jout ? Jout + (size_t)p * R * D : nullptr;
+        // residuals
+        if (ro) {
+            for (int r = g.lane; r < 3 * h->npose; r += G) ro[t.pose[r / 3].out_row + r % 3] = w.rpose[r];
+            if (h->has_limit)
+                for (int a = g.lane; a < h->na; a += G) ro[h->limit_row + a] = w.rlim[a];
+        }
+        float* S = ev.S;
+        for (int j = g.lane; j < h->nj; j += G) {
+            V3 v, om;
+            joint_subspace(t, ev.Tj, j, v, om);
+            float* s = S + 8 * j;
+            s[0] = v.x;
+            s[1] = v.y;
+            s[2] = v.z;
+            s[3] = om.x;
+            s[4] = om.y;
+            s[5] = om.z;
+        }
+        g.sync();
+        if (Jo) {
+            constexpr int PE = kChunkRows / 3;
+            for (int e0 = 0; e0 < h->npose; e0 += PE) {
+                const int ne = min(PE, h->npose - e0);
+                group_pose_rows<G>(g, t, w, ev.Tj, S, b, e0, ne);
+                for (int it = g.lane; it < 3 * ne * D; it += G) {
+                    const int rr = it / D, c = it - rr * D;
+                    const int row = t.pose[e0 + rr / 3].out_row + rr % 3;
+                    Jo[(size_t)row * D + c] = w.Jc[rr * Dp + c];
+                }
+                g.sync();
+            }
+            if (h->has_limit)
+                for (int a = g.lane; a < h->na; a += G) {
+                    const float qv = w.q[a];
+                    const float lo = t.lim[2 * a], hi = t.lim[2 * a + 1];
+                    const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
+                    Jo[(size_t)(h->limit_row + a) * D + boff + a] = t.limw[a] * sg;
+                }
+        }
+        for (int ci = 0; ci < h->ncoll; ++ci) {
+            const CollEntry& ce = t.coll[ci];
+            const int* spk = t.at<int>(ce.o_sp);
+            if (ce.mode == 0) {
+                const Slot* slots = reinterpret_cast<const Slot*>(w.raw + ce.ws_slots);
+                const int nsl = reinterpret_cast<const int*>(w.misc)[8 + ci];
+                if (ro)
+                    for (int k = g.lane; k < nsl; k += G) ro[ce.out_row + k] = slots[k].r;
+                for (int k0 = 0; Jo && k0 < nsl; k0 += kChunkRows) {
+                    const int nr = min(kChunkRows, nsl - k0);
+                    for (int r = g.lane; r < nr; r += G) {
+                        float* m = w.rowmeta + 8 * r;
+                        m[0] = __int_as_float(slots[k0 + r].i);
+                        m[1] = __int_as_float(slots[k0 + r].j);
+                        m[2] = slots[k0 + r].r;
+                        m[3] = __int_as_float(k0 + r);
+                    }
+                    g.sync();
+                    group_collision_rows<G>(g, t, w, S, b, ce, nr);
+                    for (int it = g.lane; it < nr * D; it += G) {
+                        const int rr = it / D, c = it - rr * D;
+                        Jo[(size_t)(ce.out_row + k0 + rr) * D + c] = w.Jc[rr * Dp + c];
+                    }
+                    g.sync();
+                }
+            } else {
+                for (int p0 = 0; p0 < ce.nsp; p0 += kChunkRows) {
+                    const int nr = min(kChunkRows, ce.nsp - p0);
+                    for (int r = g.lane; r < nr; r += G) {
+                        const int pk = spk[p0 + r];
+                        const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * (pk & 0xffff));
+                        const float4 bb = *reinterpret_cast<const float4*>(w.sph + 4 * (pk >> 16));
+                        const float d = norm3(V3{a.x - bb.x, a.y - bb.y, a.z - bb.z});
+                        const float pen = ce.margin - (d - a.w - bb.w);
+                        const float res = ce.weight * fmaxf(0.f, pen);
+                        float* m = w.rowmeta + 8 * r;
+                        m[0] = __int_as_float(pk & 0xffff);
+                        m[1] = __int_as_float(pk >> 16);
+                        m[2] = res;
+                        if (ro) ro[ce.out_row + p0 + r] = res;
+                    }
+                    g.sync();
+                    if (Jo) {
+                        group_collision_rows<G>(g, t, w, S, b, ce, nr);
+                        for (int it = g.lane; it < nr * D; it += G) {
+                            const int rr = it / D, c = it - rr * D;
+                            Jo[(size_t)(ce.out_row + p0 + rr) * D + c] = w.Jc[rr * Dp + c];
+                        }
+                    }
+                    g.sync();
+                }
+            }
+        }
+        g.sync();
+    }
+}
+
+// normal equations as the fused solver forms them
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) normal_kernel(const char* __restrict__ blob, int batch,
+                                                              const float* q, const float* base, float* H, float* gv,
+                                                              float* cost) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int D = h->D, T = h->T;
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        load_point<G>(g, t, w, p, q, base);
+        load_targets<G>(g, t, w, p, batch);
+        g.sync();
+        const float* b = cur_base<G>(t, w);
+        const EvalOut ev = group_eval<G>(g, t, w, w.q, b);
+        group_linearize<G>(g, t, w, ev, b);
+        if (H)
+            for (int e = g.lane; e < T; e += G) {
+                const unsigned ab = t.ab[e];
+                const int a = ab >> 8, c = ab & 0xff;
+                H[(size_t)p * D * D + a * D + c] = w.Hs[e];
+                H[(size_t)p * D * D + c * D + a] = w.Hs[e];
+            }
+        if (gv)
+            for (int i = g.lane; i < D; i += G) gv[(size_t)p * D + i] = w.Hs[T + i];
+        if (cost && g.lane == 0) cost[p] = ev.cost;
+        g.sync();
+    }
+}
+
+// damped solve on given H (full D x D), g, lambda
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) damped_solve_kernel(const char* __restrict__ blob, int batch,
+                                                                    const float* H, const float* gv,
+                                                                    const float* lambda, float* delta, float* pred,
+                                                                    int* spd) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int D = h->D, T = h->T;
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        for (int e = g.lane; e < T; e += G) {
+            const unsigned ab = t.ab[e];
+            w.Hs[e] = H[(size_t)p * D * D + (ab >> 8) * D + (ab & 0xff)];
+        }
+        for (int i = g.lane; i < D; i += G) w.Hs[T + i] = gv[(size_t)p * D + i];
+        g.sync();
+        double pr = 0.0, dn = 0.0;
+        const bool ok = group_damped_solve<G>(g, t, w, w.Hs, lambda[p], pr, dn);
+        for (int i = g.lane; i < D; i += G) delta[(size_t)p * D + i] = w.d32[i];
+        if (g.lane == 0) {
+            pred[p] = (float)pr;
+            if (spd) spd[p] = ok ? 1 : 0;
+        }
+        g.sync();
+    }
+}
+
+// one LM iteration with the reference's per-step buffers
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) step_kernel(const char* __restrict__ blob, int batch, float* q,
+                                                            float* base, float* lambda, IkLmParams P, float* cost,
+                                                            float* delta, float* pred, float* cost_new, int* accept) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    const int D = h->D;
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        load_point<G>(g, t, w, p, q, base);
+        load_targets<G>(g, t, w, p, batch);
+        g.sync();
+        LmState st;
+        group_start<G>(g, t, w, st, P);
+        st.lambda = lambda[p];
+        IkLmParams P1 = P;
+        P1.stop_rules = 0;
+        P1.max_iter = 1 << 30;
+        StepTrace tr;
+        group_iterate<G>(g, t, w, st, P1, &tr);
+        if (delta)
+            for (int i = g.lane; i < D; i += G) delta[(size_t)p * D + i] = w.d32[i];
+        if (g.lane == 0) {
+            lambda[p] = st.lambda;
+            if (cost) cost[p] = tr.accepted ? tr.cost_new : tr.cost_before;
+            if (pred) pred[p] = tr.pred;
+            if (cost_new) cost_new[p] = tr.cost_new;
+            if (accept) accept[p] = tr.accepted;
+        }
+        store_solution<G>(g, t, w, st, p, q, base, nullptr, nullptr, nullptr, nullptr);
+        g.sync();
+        w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    }
+}
+
+// IK metrics, helpers/ik/ik.py:60-82
+template <int G>
+__global__ void __launch_bounds__(kBlockThreads) metrics_kernel(const char* __restrict__ blob, int batch,
+                                                               const float* q, const float* base, int nt,
+                                                               const int* links, const float* targets, float pth,
+                                                               float rth, float* perr, float* rerr, int* success) {
+    extern __shared__ __align__(16) char smem[];
+    char* wsbase = stage_tables(blob, smem);
+    Tabs t;
+    t.bind(smem);
+    const TabHeader* h = t.h;
+    Group<G> g;
+    Ws w;
+    const int gib = threadIdx.x / G;
+    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    const int ngroups = gridDim.x * (kBlockThreads / G);
+    for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
+        load_point<G>(g, t, w, p, q, base);
+        g.sync();
+        const float* b = cur_base<G>(t, w);
+        float* Tj = group_fk<G>(g, t, w, w.q, b);
+        int ok = 1;
+        for (int i = g.lane; i < nt; i += G) {
+            const Pose L = link_pose(t, Tj, b, links[i]);
+            const Pose Tg = pose_load7(targets + ((size_t)p * nt + i) * 7);
+            // err = L^-1 o T (se3_inverse_func :70-78, se3_compose_func)
+            const V3 ti = qrot(L.w, -L.i, -L.j, -L.k, V3{L.x, L.y, L.z});
+            const Pose Li{-ti.x, -ti.y, -ti.z, L.w, -L.i, -L.j, -L.k};
+            const Pose E = compose(Li, Tg);
+            const float pe = sqrtf(E.x * E.x + E.y * E.y + E.z * E.z);
+            const float ae = 2.0f * asinf(fminf(sqrtf(E.i * E.i + E.j * E.j + E.k * E.k), 1.0f));
+            perr[(size_t)p * nt + i] = pe;
+            rerr[(size_t)p * nt + i] = ae;
+            if (pe >= pth || ae >= rth) ok = 0;
+        }
+        const unsigned bad = g.ballot(ok == 0);
+        if (g.lane == 0) success[p] = bad ? 0 : 1;
+        g.sync();
+    }
+}
+
+// integrate a tangent step, robo/robot_kernels.py:563-644 (one thread per problem)
+__global__ void integrate_kernel(int batch, int na, int floating, const float* q, const float* base,
+                                 const float* delta, const float* mask, float* qo, float* baseo) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= batch) return;
+    const int boff = floating ? 6 : 0;
+    const int D = boff + na;
+    const float* d = delta + (size_t)p * D;
+    for (int a = 0; a < na; ++a) {
+        const float m = mask ? mask[boff + a] : 1.f;
+        qo[(size_t)p * na + a] = q[(size_t)p * na + a] + m * d[boff + a];
+    }
+    if (floating) {
+        float xi[6];
+        for (int k = 0; k < 6; ++k) xi[k] = d[k];
+        if (mask)
+            for (int k = 3; k < 6; ++k) xi[k] *= mask[k];
+        const Pose B = pose_load7(base + (size_t)p * 7);
+        Pose N = compose(B, se3_exp(xi, 1e-4f));
+        if (mask) {
+            if (mask[0] == 0.f) N.x = B.x;
+            if (mask[1] == 0.f) N.y = B.y;
+            if (mask[2] == 0.f) N.z = B.z;
+        }
+        float* o = baseo + (size_t)p * 7;
+        o[0] = N.x;
+        o[1] = N.y;
+        o[2] = N.z;
+        o[3] = N.w;
+        o[4] = N.i;
+        o[5] = N.j;
+        o[6] = N.k;
+    }
+}
+
+__global__ void copy_rows_kernel(int rows, int width, const float* src, long long ss, float* dst, long long ds) {
+    const long long n = (long long)rows * width;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / width, c = i - r * width;
+        dst[r * ds + c] = src[r * ss + c];
+    }
+}
+
+__global__ void masked_copy_rows_kernel(int rows, int width, const int* mask, const float* src, float* dst) {
+    const long long n = (long long)rows * width;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / width;
+        if (mask[r] == 1) dst[i] = src[i];
+    }
+}
+
+__global__ void clamp_q_kernel(int batch, int na, float* q, const float* lim, const float* mask) {
+    const long long n = (long long)batch * na;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(i % na);
+        if (mask && mask[a] == 0.f) continue;
+        q[i] = fminf(fmaxf(q[i], lim[2 * a]), lim[2 * a + 1]);
+    }
+}
+
+// gain-ratio accept/reject on scalars, lm_optimizer.py:338-362 (FP64 ratio)
+__global__ void accept_kernel(int batch, float* cost, const float* cost_new, const float* pred, float* lambda,
+                              int* accept, IkLmParams P) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= batch) return;
+    bool acc = pred[p] > 0.f;
+    if (acc) {
+        const double rho = ((double)cost[p] - (double)cost_new[p]) / ((double)pred[p] + (double)P.gain_ratio_epsilon);
+        acc = rho >= (double)P.rho_min;
+    }
+    if (acc) {
+        accept[p] = 1;
+        lambda[p] = fmaxf(lambda[p] / P.lambda_factor, P.lambda_min);
+        cost[p] = cost_new[p];
+    } else {
+        accept[p] = 0;
+        lambda[p] = fminf(fmaxf(lambda[p] * P.lambda_factor, P.lambda_min), P.lambda_max);
+    }
+}
+
+}  // namespace b200ik

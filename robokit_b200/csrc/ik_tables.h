@@ -1,0 +1,84 @@
+// ik_tables.h — the packed table blob one IK problem class runs on.
+//
+// The host lowers a robot (RobotSpec tables, robokit robo/robot_spec.py:65-139)
+// and a term list (terms/dense/*.py) into ONE contiguous blob.  Every CTA of a
+// solver launch stages the blob into shared memory with 16-byte loads and then
+// reads the kinematic tree, the term rows and the per-group workspace layout
+// from it.  Offsets are byte offsets from the blob start, each 16-byte aligned.
+#pragma once
+#include <stdint.h>
+
+namespace b200ik {
+
+constexpr int kMaxJoints = 64;     // joint bit masks are one uint64
+constexpr int kMaxLinks = 128;
+constexpr int kMaxDim = 64;        // tangent dimension (6 base + actuated)
+constexpr int kMaxSpheres = 1024;
+constexpr int kChunkRows = 32;     // Jacobian rows staged per accumulation chunk
+
+// pose-entry kinds
+constexpr int kPosePosition = 0;
+constexpr int kPoseRotation = 1;
+
+// One block of three residual rows: a PositionTask or RotationTask frame.
+struct PoseEntry {
+    int32_t link;         // link index of the frame
+    int32_t kind;         // kPosePosition / kPoseRotation
+    int32_t term;         // term index in the user's list
+    int32_t frame;        // frame index inside the term
+    int32_t num_frames;   // frames of the owning term (target row stride)
+    int32_t out_row;      // first row in the reference layout
+    int32_t target_rows;  // rows of the target array (broadcast rule)
+    int32_t pad0;
+    float w[4];           // row weights (3 used)
+    const float* targets; // device pointer [target_rows, num_frames, 7]
+    int64_t pad1;
+};
+static_assert(sizeof(PoseEntry) == 64, "PoseEntry layout");
+
+// One SelfCollisionTask (sphere representation).
+struct CollEntry {
+    int32_t mode;         // IK_PAIRS_SLOTS / IK_PAIRS_ALL
+    int32_t K;            // slots (max_active_pairs)
+    int32_t nlp;          // link pairs
+    int32_t nsp;          // sphere pairs
+    int32_t out_row;      // first row in the reference layout
+    int32_t o_lp;         // int32 [nlp*2] link pairs
+    int32_t o_lpoff;      // int32 [nlp+1] CSR offsets into sphere pairs
+    int32_t o_sp;         // int32 [nsp] sphere pairs packed (i | j << 16)
+    int32_t ws_slots;     // workspace offset of the slot list (slots mode)
+    int32_t rows;         // residual rows this term owns in the reference layout
+    float margin;
+    float weight;
+    int32_t pad[4];
+};
+static_assert(sizeof(CollEntry) == 64, "CollEntry layout");
+
+struct TabHeader {
+    int32_t bytes;        // blob size, multiple of 16
+    int32_t nj, nl, na, ns;
+    int32_t fk_rounds;    // pointer-jumping rounds = ceil(log2(max depth))
+    int32_t D;            // tangent dimension
+    int32_t base_off;     // 6 with a floating base, else 0
+    int32_t R_ref;        // residual rows in the reference layout
+    int32_t npose, ncoll, has_limit, limit_row;
+    int32_t mask_any;     // 1 if an active-DOF mask is present
+    int32_t E;            // D(D+1)/2 + D accumulated normal-equation entries
+    int32_t T;            // D(D+1)/2
+    // robot tables
+    int32_t o_jtype, o_jparent, o_jact, o_jmimic, o_jmul, o_joff, o_jaxis, o_jpt;
+    int32_t o_lpj, o_lanc, o_lbound, o_sph, o_sphlink, o_lim;
+    int32_t o_colstart, o_coljoint, o_colmul;
+    // problem tables
+    int32_t o_pose, o_coll, o_limw, o_mask, o_ab;
+    // per-group workspace layout (byte offsets inside one group's workspace)
+    int32_t ws_bytes;
+    int32_t w_T0, w_T1, w_anc, w_sph, w_lbw, w_tgt, w_rpose, w_rlim;
+    int32_t w_Jc, w_rc, w_rowmeta, w_Hs, w_Hc, w_L, w_tmp, w_y;
+    int32_t w_q, w_qp, w_base, w_basep, w_d32, w_misc;
+    int32_t Dp;           // padded row stride of the Jacobian chunk
+    int32_t max_slots;    // sum of slot-mode K over collision terms
+    int32_t pad[4];
+};
+
+}  // namespace b200ik

@@ -1,0 +1,190 @@
+"""Pin the FP64 oracle against the reference's own golden vectors and unit-test recipes."""
+
+import numpy as np
+import pytest
+
+import oracle
+from robokit_b200.robo.robot_spec import quaternion_to_matrix
+
+
+def _pose_close(a, e, atol):
+    """Compare poses as rotation matrices + translations (quaternion sign is not unique)."""
+    return np.abs(np.asarray(a[:3]) - e[:3]).max() <= atol and np.abs(
+        quaternion_to_matrix(a[3:]) - quaternion_to_matrix(e[3:])
+    ).max() <= atol
+
+
+def test_fk_golden(panda_spec, golden):
+    """tests/robo/test_forward_kinematics.py:40-65, atol 1e-5."""
+    rob = oracle.Robot.from_spec(panda_spec)
+    checked = 0
+    for c in golden["fk"]["configurations"]:
+        q = np.array(c["qpos"], np.float32)[None]
+        base = None if c["T_world_base"] is None else np.array(c["T_world_base"], np.float32)[None]
+        out = oracle.fk(rob, q, base)
+        for lp in c["link_poses"]:
+            if lp["link_name"] not in panda_spec.link_names:
+                continue
+            li = panda_spec.link_names.index(lp["link_name"])
+            assert _pose_close(out["T_link"][0, li], np.array(lp["xyz_wxyz"]), 1e-5), (c["name"], lp["link_name"])
+            checked += 1
+    assert checked >= 40
+
+
+def test_jacobian_golden(panda_spec, golden):
+    """tests/robo/test_jacobians.py:13-66, atol 1e-5 (body and spatial, with and without a base)."""
+    rob = oracle.Robot.from_spec(panda_spec)
+    for c in golden["jacobians"]["configurations"]:
+        q = np.array(c["qpos"], np.float32)[None]
+        base = None if c["T_world_base"] is None else np.array(c["T_world_base"], np.float32)[None]
+        for lj in c["link_jacobians"]:
+            if lj["link_name"] not in panda_spec.link_names:
+                continue
+            li = panda_spec.link_names.index(lj["link_name"])
+            for frame in ("body", "spatial"):
+                J = oracle.link_jacobian(rob, q, base, li, frame == "body")[0]
+                e = np.array(lj[f"{frame}_J_joints"])
+                if base is not None:
+                    e = np.concatenate([np.array(lj[f"{frame}_J_base"]), e], axis=1)
+                np.testing.assert_allclose(J, e, atol=1e-5, err_msg=f"{c['name']} {lj['link_name']} {frame}")
+
+
+def test_fk_doctest_panda_hand(panda_spec):
+    """robo/robot.py:41-44 and :147-154 known answers (atol 1e-4)."""
+    rob = oracle.Robot.from_spec(panda_spec)
+    q = np.array([[0.0, -1.2, 0.0, -2.0, 0.0, 1.0, 0.0, 0.0]], np.float32)
+    hand = panda_spec.link_names.index("panda_hand")
+    out = oracle.fk(rob, q)
+    assert _pose_close(out["T_link"][0, hand], np.array([6.0860e-02, -4.7547e-12, 7.6373e-01, 0.0382, 0.9193,
+                                                          0.3808, 0.0922]), 1e-4)
+    base = np.array([[1.0, 2.0, 3.0, 0.7071, 0.0, 0.7071, 0.0]], np.float32)
+    out = oracle.fk(rob, q, base)
+    assert _pose_close(out["T_link"][0, hand], np.array([1.76371783, 2.0, 2.93915576, -0.24222432, 0.71524162,
+                                                          0.29626278, -0.58478125]), 1e-3)
+
+
+def test_accept_reject_kats():
+    """tests/opt/test_optimizer_acceptance.py:41-69 (rho_min 1e-3, eps 1e-8, factor 2, lambda in [1e-6, 1e6])."""
+    prm = oracle.params(lambda_factor=2.0, lambda_min=1e-6, lambda_max=1e6, rho_min=1e-3, gain_ratio_epsilon=1e-8)
+    cost, lam, acc = oracle.accept_reject([1.0, 1.0, 1.0], [1.1, 0.8, 0.8], [-0.05, -0.05, 0.2], [1.0, 1.0, 1.0], prm)
+    assert list(acc) == [0, 0, 1]
+    np.testing.assert_allclose(cost, [1.0, 1.0, 0.8])
+    np.testing.assert_allclose(lam, [2.0, 2.0, 0.5])
+
+
+def test_damped_solve_matches_numpy():
+    """lm_optimizer.py:56-79 vs np.linalg.solve (tests/opt/test_optimizer.py:574-597 recipe)."""
+    rng = np.random.default_rng(0)
+    for D in (7, 26, 35, 64):
+        A = rng.normal(size=(4, D, D))
+        H = A @ A.transpose(0, 2, 1) + 0.3 * np.eye(D)
+        g = rng.normal(size=(4, D))
+        lam = np.array([0.01, 1.0, 1000.0, 1e5])
+        delta, pred, spd = oracle.damped_solve(H, g, lam)
+        exp = np.linalg.solve(H + lam[:, None, None] * np.eye(D), -g[..., None])[..., 0]
+        np.testing.assert_allclose(delta, exp, rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(pred, 0.5 * np.sum(exp * (lam[:, None] * exp - g), 1), rtol=1e-9)
+        assert spd.all()
+    # an indefinite matrix is reported, with a zero step
+    H = -np.eye(3)[None]
+    delta, pred, spd = oracle.damped_solve(H, np.ones((1, 3)), np.array([1e-5]))
+    assert spd[0] == 0 and np.all(delta == 0) and pred[0] == 0
+
+
+def test_masked_step_matches_reduced_problem(panda_spec):
+    """tests/opt/test_optimizer.py:366-429: the mask zeroes J columns before forming J^T J."""
+    rob = oracle.Robot.from_spec(panda_spec)
+    hand = panda_spec.link_names.index("panda_hand")
+    q = panda_spec.midrange_q[None].astype(np.float32)
+    tgt = np.array([[[0.4, 0.1, 0.5, 1.0, 0.0, 0.0, 0.0]]], np.float32)
+    terms = oracle.Terms([
+        dict(kind=1, num_frames=1, frame_links=[hand], weights=[10.0] * 3, targets=tgt, target_rows=1),
+        dict(kind=2, num_frames=1, frame_links=[hand], weights=[2.0] * 3, targets=tgt, target_rows=1),
+    ])
+    D = panda_spec.num_actuated_joints
+    mask = np.ones(D, np.float32)
+    mask[1] = 0.0
+    r, J = oracle.residual_jacobian(rob, terms, q)
+    Jm = J[0] * mask[None]
+    lam = 1e-2
+    exp = np.linalg.solve(Jm.T @ Jm + lam * np.eye(D), -(Jm.T @ r[0]))
+    H, g, cost = oracle.normal_equations(rob, terms, q, None, mask)
+    delta, pred, spd = oracle.damped_solve(H, g, np.array([lam]))
+    assert abs(delta[0, 1]) < 1e-12
+    np.testing.assert_allclose(delta[0], exp, rtol=1e-8, atol=1e-10)
+    np.testing.assert_allclose(cost[0], 0.5 * r[0] @ r[0])
+
+
+def test_oracle_jacobian_matches_finite_differences(panda_collision_spec):
+    """The analytic Jacobian of every term kind vs central differences of the residuals."""
+    from robokit_b200.robo.robot_spec import collision_pair_tables
+
+    spec = panda_collision_spec
+    rob = oracle.Robot.from_spec(spec)
+    hand = spec.link_names.index("panda_hand")
+    pairs, lp, off, grouped = collision_pair_tables(spec)
+    tgt = np.array([[[0.3, -0.2, 0.6, 0.9, 0.1, 0.3, 0.2]]], np.float32)
+    tgt[..., 3:] /= np.linalg.norm(tgt[..., 3:])
+    for mode in (0, 1):
+        terms = oracle.Terms([
+            dict(kind=1, num_frames=1, frame_links=[hand], weights=[2.0, 3.0, 4.0], targets=tgt, target_rows=1),
+            dict(kind=2, num_frames=1, frame_links=[hand], weights=[1.0, 1.5, 0.5], targets=tgt, target_rows=1),
+            dict(kind=3, weights=np.full(spec.num_actuated_joints, 2.0)),
+            dict(kind=4, weights=[1.5], margin=0.5, max_active_pairs=50, pair_mode=mode,
+                 num_link_pairs=len(lp), link_pairs=lp.ravel(), link_pair_offsets=off,
+                 num_sphere_pairs=len(grouped), sphere_pairs=grouped.ravel()),
+        ])
+        rng = np.random.default_rng(7)
+        q = (spec.midrange_q + rng.normal(0, 0.15, spec.num_actuated_joints)).astype(np.float64)
+        base = np.array([[0.1, -0.2, 0.3, 0.9, 0.1, -0.3, 0.2]])
+        base[:, 3:] /= np.linalg.norm(base[:, 3:])
+        _, J = oracle.residual_jacobian(rob, terms, q[None].astype(np.float32), base.astype(np.float32))
+        # joint columns: float32 inputs limit the difference step
+        eps = 1e-3
+        fd = np.zeros_like(J[0])
+        kink = np.zeros(J.shape[1], bool)  # hinge rows whose activity changes inside the stencil
+        nlim = spec.num_actuated_joints
+        stable = np.ones(J.shape[2], bool)  # columns whose slot selection is the same on both sides
+        for a in range(spec.num_actuated_joints):
+            qp, qm = q.copy(), q.copy()
+            qp[a] += eps
+            qm[a] -= eps
+            rp, _ = oracle.residual_jacobian(rob, terms, qp[None].astype(np.float32), base.astype(np.float32))
+            rm, _ = oracle.residual_jacobian(rob, terms, qm[None].astype(np.float32), base.astype(np.float32))
+            fd[:, 6 + a] = (rp[0] - rm[0]) / (2 * eps)
+            kink |= (rp[0] == 0) != (rm[0] == 0)
+            if mode == 0:
+                sp, sm = rp[0][6 + nlim:], rm[0][6 + nlim:]
+                stable[6 + a] = np.count_nonzero(sp) == np.count_nonzero(sm) and np.max(np.abs(sp - sm)) < 0.05
+        if mode == 1:
+            fd[kink] = J[0][kink]
+        # rotation rows use the reference's approximate Jacobian (no SO(3) J_l^-1 factor,
+        # rotation_task.py:374-390); compare position, limit and collision rows exactly
+        rows = np.r_[0:3, 6:J.shape[1]]
+        if mode == 0:
+            # slot rows follow the selection order: compare column sums where the selection is stable
+            # (tests/terms/test_self_collision_task.py:124-157 compares sums likewise)
+            rows = np.r_[0:3, 6:6 + nlim]
+            cols = np.nonzero(stable[6:])[0] + 6
+            assert len(cols) >= 4
+            np.testing.assert_allclose(J[0][6 + nlim:, cols].sum(0), fd[6 + nlim:, cols].sum(0), atol=2e-2)
+        np.testing.assert_allclose(J[0][rows][:, 6:], fd[rows][:, 6:], atol=2e-2)
+
+
+def test_oracle_lm_reaches_reachable_targets():
+    """A small C1 batch: LM from random starts reaches most FK targets."""
+    from robokit_b200 import configs
+
+    cfg = configs.make("chain7", 128, seed=3)
+    rob = oracle.Robot.from_spec(cfg.workload.spec)
+    terms = oracle.Terms(configs.oracle_terms(cfg))
+    prm = oracle.params(max_iter=50, lambda_init=1e-3, lambda_factor=10.0)
+    out = oracle.solve(rob, terms, prm, cfg.workload.q0, threads=4)
+    pe, re, ok = oracle.metrics(rob, out["q"], None, cfg.workload.target_links, cfg.workload.targets, 1e-3, 0.01)
+    assert ok.mean() > 0.6
+    # start cost never increases (accepted steps only decrease the cost)
+    H, g, c0 = oracle.normal_equations(rob, terms, cfg.workload.q0)
+    assert np.all(out["cost"] <= c0 + 1e-12)
+    # multithreaded and single-threaded solves agree exactly
+    out1 = oracle.solve(rob, terms, prm, cfg.workload.q0, threads=1)
+    np.testing.assert_array_equal(out1["q"], out["q"])
