@@ -45,6 +45,8 @@ extern "C" {
 #define IK_ST_MAX_ITER 2    /* iteration cap reached                          */
 #define IK_ST_NOT_SPD 4     /* some damped normal matrix had a pivot <= 0     */
 #define IK_ST_NONFINITE 8   /* non-finite cost at the start point             */
+#define IK_ST_FLAGS 0xff    /* status bits; the rest counts accepted steps    */
+#define IK_ST_ACCEPTS(s) ((s) >> 8)
 
 /* joint types, robo/robot_spec.py:34-41 */
 #define IK_JOINT_FIXED 0
@@ -163,7 +165,8 @@ int ik_problem_set_targets(IkProblem* problem, int32_t term_index, const float* 
  * opt/lm_optimizer.py:834-1005).  d_q [batch*na] and d_base [batch*7] (NULL
  * without a floating base) are read as the start point and overwritten with
  * the solution.  Outputs: d_cost [batch] final cost 0.5*|r|^2, d_lambda [batch]
- * final damping, d_iters [batch] iterations run, d_status [batch] IK_ST_* bits.
+ * final damping, d_iters [batch] iterations run, d_status [batch] IK_ST_* bits
+ * in bits 0-7 and the number of accepted steps in bits 8-31 (IK_ST_ACCEPTS).
  * Any output may be NULL. */
 int ik_solve_plain(IkProblem* problem, int32_t batch, float* d_q, float* d_base, const IkLmParams* params,
                    float* d_cost, float* d_lambda, int32_t* d_iters, int32_t* d_status, void* stream);
@@ -267,6 +270,10 @@ int ik_event_record(void* event, void* stream);
 int ik_event_elapsed_ms(void* start, void* stop, float* ms);
 /* Count of this library's kernel launches since load (for launch accounting). */
 int ik_launch_count(int64_t* out);
+/* Measured CUDA-core FMA throughput (fp64 = 0: FP32, 1: FP64) in TFLOP/s on
+ * the current device; independent FMA chains on every SM, best of 3 timed
+ * launches.  The roofline denominator of the IK kernels.  Synchronises. */
+int ik_measure_fma_peak(int32_t fp64, float* tflops);
 
 #ifdef __cplusplus
 }

@@ -187,6 +187,7 @@ _SIGNATURES = {
     "ik_event_record": (ctypes.c_int, [_vp, _vp]),
     "ik_event_elapsed_ms": (ctypes.c_int, [_vp, _vp, _f32p]),
     "ik_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int64)]),
+    "ik_measure_fma_peak": (ctypes.c_int, [ctypes.c_int32, _f32p]),
 }
 
 _lib: Optional[ctypes.CDLL] = None

@@ -1065,6 +1065,36 @@ int ik_integrate(int32_t batch, int32_t num_actuated, int32_t floating_base, con
     return check_launch();
 }
 
+int ik_measure_fma_peak(int32_t fp64, float* tflops) {
+    if (!tflops) return fail(IK_E_INVALID, "out is NULL");
+    const int blocks = num_sms() * 8, threads = 256;
+    const int iters = fp64 ? 2048 : 4096;
+    void* out = nullptr;
+    CK(cudaMalloc(&out, blocks * sizeof(double)));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        CK(cudaEventRecord(a, 0));
+        if (fp64)
+            fma_peak_kernel<double><<<blocks, threads>>>((double*)out, iters);
+        else
+            fma_peak_kernel<float><<<blocks, threads>>>((float*)out, iters);
+        CK(cudaEventRecord(b, 0));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        if (rep > 0) best = std::min(best, ms);  // first launch is warm-up
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    const double flops = 2.0 * 32.0 * iters * (double)blocks * threads;
+    *tflops = (float)(flops / (best * 1e-3) / 1e12);
+    return IK_OK;
+}
+
 static int elementwise_grid(long long n) {
     long long g = (n + 255) / 256;
     if (g < 1) g = 1;

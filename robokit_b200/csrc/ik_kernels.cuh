@@ -18,7 +18,7 @@ __host__ __device__ inline int rec_stride(int E) { return ((E + 8) + 3) & ~3; }
 // per-problem solver state kept in registers (identical in every lane of the group)
 struct LmState {
     float cost, lambda, pos_err, rot_err;
-    int status, iters;
+    int status, iters, accepts;
 };
 
 // Stage the table blob into shared memory; returns the start of group workspaces.
@@ -79,6 +79,7 @@ __device__ void group_start(const Group<G>& g, const Tabs& t, Ws& w, LmState& st
     st.lambda = P.lambda_init;
     st.status = isfinite(ev.cost) ? IK_ST_RUNNING : IK_ST_NONFINITE;
     st.iters = 0;
+    st.accepts = 0;
     group_linearize<G>(g, t, w, ev, cur_base<G>(t, w));
 }
 
@@ -125,6 +126,7 @@ __device__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& 
         st.pos_err = ev.max_pos;
         st.rot_err = ev.max_rot;
         st.lambda = fmaxf(st.lambda / P.lambda_factor, P.lambda_min);
+        st.accepts += 1;
         group_linearize<G>(g, t, w, ev, floating ? w.base : nullptr);
     } else {
         st.lambda = fminf(fmaxf(st.lambda * P.lambda_factor, P.lambda_min), P.lambda_max);
@@ -148,7 +150,7 @@ __device__ void store_solution(const Group<G>& g, const Tabs& t, const Ws& w, co
         if (cost) cost[p] = st.cost;
         if (lambda) lambda[p] = st.lambda;
         if (iters) iters[p] = st.iters;
-        if (status) status[p] = st.status;
+        if (status) status[p] = (st.status & IK_ST_FLAGS) | (st.accepts << 8);
     }
 }
 
@@ -205,6 +207,7 @@ __global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __r
             st.rot_err = s.rot_err;
             st.status = s.status;
             st.iters = s.iters;
+            st.accepts = s.pad0;
             const bool done = (st.status & (IK_ST_CONVERGED | IK_ST_MAX_ITER | IK_ST_NONFINITE)) != 0;
             touched = !done;
             if (!done) {
@@ -226,7 +229,8 @@ __global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __r
             s.rot_err = st.rot_err;
             s.status = st.status;
             s.iters = st.iters;
-            s.pad0 = s.pad1 = 0;
+            s.pad0 = st.accepts;
+            s.pad1 = 0;
             *rsc = s;
         }
         store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
@@ -735,6 +739,27 @@ __global__ void integrate_kernel(int batch, int na, int floating, const float* q
         o[5] = N.j;
         o[6] = N.k;
     }
+}
+
+// Independent FMA chains per thread: the CUDA-core FP32 / FP64 throughput the
+// roofline of the (non-tensor) IK kernels is stated against.
+template <typename T>
+__global__ void fma_peak_kernel(T* out, int iters) {
+    T a[8];
+    const T b = (T)0.9999999, c = (T)1e-7;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = (T)(threadIdx.x + k);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+        }
+    }
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == (T)-1) out[blockIdx.x] = s;  // keeps the chains live
 }
 
 __global__ void copy_rows_kernel(int rows, int width, const float* src, long long ss, float* dst, long long ds) {
