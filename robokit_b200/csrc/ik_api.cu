@@ -144,7 +144,7 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_rlim = take(na * 4);
     h->w_Jc = take(kChunkRows * h->Dp * 4);
     h->w_rc = take(kChunkRows * 4);
-    h->w_rowmeta = take(kChunkRows * 8 * 4);
+    h->w_rowmeta = take(kChunkRows * 4 * 4);
     h->w_Hs = take(h->E * 4);
     h->w_Hc = take(h->E * 4);
     h->w_L = take(h->T * 8);
@@ -530,7 +530,10 @@ int build_problem_blob(IkProblem* P) {
         c.o_lpoff = b.addv(th.lpoff);
         c.o_sp = b.addv(th.sp);
         coll_slot_rel.push_back(slot_bytes);
-        if (c.mode == IK_PAIRS_SLOTS) slot_bytes += al16(std::min(c.K, std::max(c.nlp, 1)) * (int)sizeof(Slot));
+        if (c.mode == IK_PAIRS_SLOTS)
+            slot_bytes += al16(std::min(c.K, std::max(c.nlp, 1)) * (int)sizeof(Slot));
+        else  // candidate link pairs (pruned scan) or one activity mask per lane (flat scan)
+            slot_bytes += al16(std::max(std::max(c.nlp, 1) * (int)sizeof(int), 32 * (int)sizeof(unsigned long long)));
         coll.push_back(c);
     }
     int max_slots = 0;
@@ -552,7 +555,7 @@ int build_problem_blob(IkProblem* P) {
     h = b.hdr();
     h->ncoll = (int)coll.size();
     h->max_slots = max_slots;
-    const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0, max_slots > 0);
+    const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0, h->ncoll > 0);
     CollEntry* ce = reinterpret_cast<CollEntry*>(b.buf.data() + o_coll);
     for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
     h->bytes = (int)b.buf.size();

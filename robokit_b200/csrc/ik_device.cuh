@@ -14,6 +14,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <utility>
+#include <type_traits>
 #include "ik_tables.h"
 
 namespace b200ik {
@@ -117,18 +119,21 @@ __device__ __forceinline__ Pose se3_exp(const float xi[6], float eps) {
     return Pose{tr.x, tr.y, tr.z, qw, qi, qj, qk};
 }
 
-// axis-angle of a standardised quaternion, quaternion_to_axis_angle_func :228-247
-__device__ __forceinline__ V3 quat_to_axis_angle(float w, float i, float j, float k) {
-    const float n = sqrtf(i * i + j * j + k * k);
+// axis-angle of a standardised quaternion, quaternion_to_axis_angle_func :228-247.
+// With half = atan2(n, w), sin(half) = n / |q| exactly, which replaces the sine;
+// `angle` (2 half) is the rotation angle.
+__device__ __forceinline__ V3 quat_to_axis_angle(float w, float i, float j, float k, float& angle) {
+    const float n2 = i * i + j * j + k * k;
+    const float n = sqrtf(n2);
     const float half = atan2f(n, w);
-    const float angle = 2.0f * half;
-    float s;
+    angle = 2.0f * half;
+    float inv_s;  // 1 / (sin(half) / angle)
     if (fabsf(angle) < 1e-6f) {
-        s = 0.5f - angle * angle / 48.0f;
+        inv_s = 1.0f / (0.5f - angle * angle / 48.0f);
     } else {
-        s = sinf(half) / angle;
+        inv_s = angle * sqrtf(n2 + w * w) / n;
     }
-    return V3{i / s, j / s, k / s};
+    return V3{i * inv_s, j * inv_s, k * inv_s};
 }
 
 // ---------------------------------------------------------------------------
@@ -194,111 +199,84 @@ __device__ __forceinline__ float group_ksum(const Group<G>& g, float s, float c)
 // ---------------------------------------------------------------------------
 // table / workspace views
 // ---------------------------------------------------------------------------
+// Table view: only the blob base is held; every sub-array is derived from the
+// header's offsets (shared memory) where it is used, so the compiler can
+// rematerialise addresses instead of pinning dozens of pointers in registers.
+#define IK_TAB(type, name, field) \
+    __device__ __forceinline__ const type* name() const { return reinterpret_cast<const type*>(base + h->field); }
 struct Tabs {
     const TabHeader* h;
-    const int* jtype;
-    const int* jparent;
-    const int* jact;
-    const int* jmimic;
-    const float* jmul;
-    const float* joff;
-    const float* jaxis;  // [nj*4]
-    const float* jpt;    // [nj*8]
-    const int* lpj;
-    const unsigned long long* lanc;
-    const float* lbound;  // [nl*4]
-    const float* sph;     // [ns*4]
-    const int* sphlink;
-    const float* lim;     // [na*2]
-    const int* colstart;
-    const int* coljoint;
-    const float* colmul;
-    const PoseEntry* pose;
-    const CollEntry* coll;
-    const float* limw;
-    const float* mask;
-    const uint16_t* ab;
     const char* base;
     __device__ __forceinline__ void bind(const char* blob) {
         base = blob;
         h = reinterpret_cast<const TabHeader*>(blob);
-        jtype = reinterpret_cast<const int*>(blob + h->o_jtype);
-        jparent = reinterpret_cast<const int*>(blob + h->o_jparent);
-        jact = reinterpret_cast<const int*>(blob + h->o_jact);
-        jmimic = reinterpret_cast<const int*>(blob + h->o_jmimic);
-        jmul = reinterpret_cast<const float*>(blob + h->o_jmul);
-        joff = reinterpret_cast<const float*>(blob + h->o_joff);
-        jaxis = reinterpret_cast<const float*>(blob + h->o_jaxis);
-        jpt = reinterpret_cast<const float*>(blob + h->o_jpt);
-        lpj = reinterpret_cast<const int*>(blob + h->o_lpj);
-        lanc = reinterpret_cast<const unsigned long long*>(blob + h->o_lanc);
-        lbound = reinterpret_cast<const float*>(blob + h->o_lbound);
-        sph = reinterpret_cast<const float*>(blob + h->o_sph);
-        sphlink = reinterpret_cast<const int*>(blob + h->o_sphlink);
-        lim = reinterpret_cast<const float*>(blob + h->o_lim);
-        colstart = reinterpret_cast<const int*>(blob + h->o_colstart);
-        coljoint = reinterpret_cast<const int*>(blob + h->o_coljoint);
-        colmul = reinterpret_cast<const float*>(blob + h->o_colmul);
-        pose = reinterpret_cast<const PoseEntry*>(blob + h->o_pose);
-        coll = reinterpret_cast<const CollEntry*>(blob + h->o_coll);
-        limw = reinterpret_cast<const float*>(blob + h->o_limw);
-        mask = reinterpret_cast<const float*>(blob + h->o_mask);
-        ab = reinterpret_cast<const uint16_t*>(blob + h->o_ab);
     }
+    IK_TAB(int, jtype, o_jtype)
+    IK_TAB(int, jparent, o_jparent)
+    IK_TAB(int, jact, o_jact)
+    IK_TAB(int, jmimic, o_jmimic)
+    IK_TAB(float, jmul, o_jmul)
+    IK_TAB(float, joff, o_joff)
+    IK_TAB(float, jaxis, o_jaxis)    // [nj*4]
+    IK_TAB(float, jpt, o_jpt)        // [nj*8]
+    IK_TAB(int, lpj, o_lpj)
+    IK_TAB(unsigned long long, lanc, o_lanc)
+    IK_TAB(float, lbound, o_lbound)  // [nl*4]
+    IK_TAB(float, sph, o_sph)        // [ns*4]
+    IK_TAB(int, sphlink, o_sphlink)
+    IK_TAB(float, lim, o_lim)        // [na*2]
+    IK_TAB(int, colstart, o_colstart)
+    IK_TAB(int, coljoint, o_coljoint)
+    IK_TAB(float, colmul, o_colmul)
+    IK_TAB(PoseEntry, pose, o_pose)
+    IK_TAB(CollEntry, coll, o_coll)
+    IK_TAB(float, limw, o_limw)
+    IK_TAB(float, mask, o_mask)
+    IK_TAB(uint16_t, ab, o_ab)
     template <typename T>
     __device__ __forceinline__ const T* at(int off) const { return reinterpret_cast<const T*>(base + off); }
 };
+#undef IK_TAB
 
+// Per-group workspace view: the current / proposed joint and base buffers are
+// held (the accept path swaps them); the rest is derived from header offsets.
+#define IK_WS(type, name, field) \
+    __device__ __forceinline__ type* name() const { return reinterpret_cast<type*>(raw + h->field); }
 struct Ws {
-    float* T0;      // FK buffer A [nj*8]
-    float* T1;      // FK buffer B [nj*8] / motion subspace
-    int* anc;       // [2*nj]
-    float* sph;     // world spheres [ns*4]
-    float* lbw;     // world link bounding centres [nl*4]
-    float* tgt;     // pose targets [npose*8]
-    float* rpose;   // pose residuals [npose*3]
-    float* rlim;    // limit residuals [na]
-    float* Jc;      // Jacobian chunk [kChunkRows*Dp]
-    float* rc;      // chunk residuals [kChunkRows]
-    float* rowmeta; // chunk row metadata [kChunkRows*8]
-    float* Hs;      // normal equations [E] (packed lower H, then g)
-    float* Hc;      // compensation terms [E]
-    double* L;      // Cholesky factor [T]
-    double* tmp;    // [D]
-    double* y;      // [D] solve vector / step
-    float* q;       // current joints [na]
-    float* qp;      // proposed joints [na]
-    float* base;    // current base pose [8]
-    float* basep;   // proposed base pose [8]
-    float* d32;     // step in FP32 [D]
-    float* misc;    // [16]
     char* raw;
-    __device__ __forceinline__ void bind(char* w, const TabHeader* h) {
+    const TabHeader* h;
+    float* q;      // current joints [na]
+    float* qp;     // proposed joints [na]
+    float* base;   // current base pose [8]
+    float* basep;  // proposed base pose [8]
+    __device__ __forceinline__ void bind(char* w, const TabHeader* hh) {
         raw = w;
-        T0 = reinterpret_cast<float*>(w + h->w_T0);
-        T1 = reinterpret_cast<float*>(w + h->w_T1);
-        anc = reinterpret_cast<int*>(w + h->w_anc);
-        sph = reinterpret_cast<float*>(w + h->w_sph);
-        lbw = reinterpret_cast<float*>(w + h->w_lbw);
-        tgt = reinterpret_cast<float*>(w + h->w_tgt);
-        rpose = reinterpret_cast<float*>(w + h->w_rpose);
-        rlim = reinterpret_cast<float*>(w + h->w_rlim);
-        Jc = reinterpret_cast<float*>(w + h->w_Jc);
-        rc = reinterpret_cast<float*>(w + h->w_rc);
-        rowmeta = reinterpret_cast<float*>(w + h->w_rowmeta);
-        Hs = reinterpret_cast<float*>(w + h->w_Hs);
-        Hc = reinterpret_cast<float*>(w + h->w_Hc);
-        L = reinterpret_cast<double*>(w + h->w_L);
-        tmp = reinterpret_cast<double*>(w + h->w_tmp);
-        y = reinterpret_cast<double*>(w + h->w_y);
+        h = hh;
         q = reinterpret_cast<float*>(w + h->w_q);
         qp = reinterpret_cast<float*>(w + h->w_qp);
         base = reinterpret_cast<float*>(w + h->w_base);
         basep = reinterpret_cast<float*>(w + h->w_basep);
-        d32 = reinterpret_cast<float*>(w + h->w_d32);
-        misc = reinterpret_cast<float*>(w + h->w_misc);
     }
+    IK_WS(float, T0, w_T0)            // FK buffer A [nj*8]
+    IK_WS(float, T1, w_T1)            // FK buffer B [nj*8] / motion subspace
+    IK_WS(int, anc, w_anc)            // [2*nj]
+    IK_WS(float, sph, w_sph)          // world spheres [ns*4]
+    IK_WS(float, lbw, w_lbw)          // world link bounding centres [nl*4]
+    IK_WS(float, tgt, w_tgt)          // pose targets [npose*8]
+    IK_WS(float, rpose, w_rpose)      // pose residuals [npose*3]
+    IK_WS(float, rlim, w_rlim)        // limit residuals [na]
+    IK_WS(float, Jc, w_Jc)            // Jacobian chunk [kChunkRows*Dp]
+    IK_WS(float, rc, w_rc)            // chunk residuals [kChunkRows]
+    IK_WS(float, rowmeta, w_rowmeta)  // chunk row metadata [kChunkRows*4]: sphere i, sphere j, residual, spare
+    IK_WS(float, Hs, w_Hs)            // normal equations [E] (packed lower H, then g)
+    IK_WS(float, Hc, w_Hc)            // compensation terms [E]
+    IK_WS(double, L, w_L)             // Cholesky factor [T]
+    IK_WS(double, tmp, w_tmp)         // [D]
+    IK_WS(double, y, w_y)             // [D]
+    IK_WS(float, d32, w_d32)          // step in FP32 [D]
+    IK_WS(float, misc, w_misc)        // [64]
 };
+#undef IK_WS
 
 // slot record of the slots-mode self-collision term: sphere pair + residual
 struct Slot {
@@ -313,23 +291,23 @@ struct Slot {
 // T_world_joint; the other FK buffer is free afterwards.
 // ---------------------------------------------------------------------------
 template <int G>
-__device__ float* group_fk(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
+__device__ __forceinline__ float* group_fk(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
     const int nj = t.h->nj;
-    float* src = w.T0;
-    float* dst = w.T1;
-    int* asrc = w.anc;
-    int* adst = w.anc + nj;
+    float* src = w.T0();
+    float* dst = w.T1();
+    int* asrc = w.anc();
+    int* adst = w.anc() + nj;
     for (int j = g.lane; j < nj; j += G) {
         float pos = 0.f;
-        const int mim = t.jmimic[j];
-        const int act = t.jact[j];
+        const int mim = t.jmimic()[j];
+        const int act = t.jact()[j];
         if (mim >= 0)
-            pos = q[mim] * t.jmul[j] + t.joff[j];
+            pos = q[mim] * t.jmul()[j] + t.joff()[j];
         else if (act >= 0)
             pos = q[act];
-        const Pose P = pose_load(t.jpt + 8 * j);
-        const int ty = t.jtype[j];
-        const float ax = t.jaxis[4 * j], ay = t.jaxis[4 * j + 1], az = t.jaxis[4 * j + 2];
+        const Pose P = pose_load(t.jpt() + 8 * j);
+        const int ty = t.jtype()[j];
+        const float ax = t.jaxis()[4 * j], ay = t.jaxis()[4 * j + 1], az = t.jaxis()[4 * j + 2];
         Pose X;
         if (ty == 2) {
             float s, c;
@@ -341,7 +319,7 @@ __device__ float* group_fk(const Group<G>& g, const Tabs& t, Ws& w, const float*
             X = P;
         }
         pose_store(src + 8 * j, X);
-        asrc[j] = t.jparent[j];
+        asrc[j] = t.jparent()[j];
     }
     g.sync();
     const int rounds = t.h->fk_rounds;
@@ -374,19 +352,19 @@ __device__ float* group_fk(const Group<G>& g, const Tabs& t, Ws& w, const float*
 }
 
 __device__ __forceinline__ Pose link_pose(const Tabs& t, const float* Tj, const float* base, int link) {
-    const int j = t.lpj[link];
+    const int j = t.lpj()[link];
     if (j >= 0) return pose_load(Tj + 8 * j);
     return base ? pose_load(base) : pose_identity();
 }
 
 // world motion subspace column of joint j: [v; w] = Ad(T_world_joint) twist_j
 __device__ __forceinline__ void joint_subspace(const Tabs& t, const float* Tj, int j, V3& v, V3& om) {
-    const int ty = t.jtype[j];
+    const int ty = t.jtype()[j];
     v = V3{0.f, 0.f, 0.f};
     om = V3{0.f, 0.f, 0.f};
     if (ty == 0) return;
     const Pose P = pose_load(Tj + 8 * j);
-    const V3 a{t.jaxis[4 * j], t.jaxis[4 * j + 1], t.jaxis[4 * j + 2]};
+    const V3 a{t.jaxis()[4 * j], t.jaxis()[4 * j + 1], t.jaxis()[4 * j + 2]};
     const V3 Ra = qrot(P.w, P.i, P.j, P.k, a);
     if (ty == 2) {
         om = Ra;
@@ -417,11 +395,11 @@ __device__ __forceinline__ void column_twist(const Tabs& t, const float* S, cons
     const int a = c - boff;
     v = V3{0.f, 0.f, 0.f};
     om = V3{0.f, 0.f, 0.f};
-    const unsigned long long anc = t.lanc[link];
-    for (int idx = t.colstart[a]; idx < t.colstart[a + 1]; ++idx) {
-        const int j = t.coljoint[idx];
+    const unsigned long long anc = t.lanc()[link];
+    for (int idx = t.colstart()[a]; idx < t.colstart()[a + 1]; ++idx) {
+        const int j = t.coljoint()[idx];
         if ((anc >> j) & 1ull) {
-            const float m = t.colmul[idx];
+            const float m = t.colmul()[idx];
             const float* s = S + 8 * j;
             v = v + m * V3{s[0], s[1], s[2]};
             om = om + m * V3{s[3], s[4], s[5]};
@@ -442,10 +420,10 @@ __device__ __forceinline__ float collision_column(const Tabs& t, const float* S,
         return dot(n, cross(om, ci - cj));
     }
     const int a = c - boff;
-    const unsigned long long ai = t.lanc[li], aj = t.lanc[lj];
+    const unsigned long long ai = t.lanc()[li], aj = t.lanc()[lj];
     float val = 0.f;
-    for (int idx = t.colstart[a]; idx < t.colstart[a + 1]; ++idx) {
-        const int j = t.coljoint[idx];
+    for (int idx = t.colstart()[a]; idx < t.colstart()[a + 1]; ++idx) {
+        const int j = t.coljoint()[idx];
         const bool bi = (ai >> j) & 1ull, bj = (aj >> j) & 1ull;
         if (!bi && !bj) continue;
         const float* s = S + 8 * j;
@@ -453,9 +431,91 @@ __device__ __forceinline__ float collision_column(const Tabs& t, const float* S,
         V3 col_i{0.f, 0.f, 0.f}, col_j{0.f, 0.f, 0.f};
         if (bi) col_i = v + cross(om, ci);
         if (bj) col_j = v + cross(om, cj);
-        val += t.colmul[idx] * dot(n, col_i - col_j);
+        val += t.colmul()[idx] * dot(n, col_i - col_j);
     }
     return val;
+}
+
+// ---------------------------------------------------------------------------
+// Broad phase of a collision term: link pairs whose bounding spheres come
+// within the margin (+ `inflate`), in link-pair order, into `list` (at most
+// `cap`).  With inflate = 0 and the exact distance this is the reference's
+// selection test (self_collision_task.py:73-87); the all-pairs mode uses a
+// small positive inflate, which keeps every sphere pair that can penetrate
+// (a link's bounding sphere contains its spheres).  Returns the count.
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ __forceinline__ int group_broad_phase(const Group<G>& g, const Tabs& t, const Ws& w, const CollEntry& ce, int* list,
+                                 int stride, int cap, bool exact) {
+    const int* lp = t.at<int>(ce.o_lp);
+    int count = 0;
+    for (int b0 = 0; b0 < ce.nlp; b0 += G) {
+        const int l = b0 + g.lane;
+        bool act = false;
+        if (l < ce.nlp) {
+            const float4 a = *reinterpret_cast<const float4*>(w.lbw() + 4 * lp[2 * l]);
+            const float4 b = *reinterpret_cast<const float4*>(w.lbw() + 4 * lp[2 * l + 1]);
+            const V3 d{a.x - b.x, a.y - b.y, a.z - b.z};
+            if (exact) {
+                act = (a.w + b.w + ce.margin - norm3(d)) > 0.f;
+            } else {
+                const float thr = a.w + b.w + ce.margin + 1e-5f;
+                act = thr > 0.f && dot(d, d) < thr * thr;
+            }
+        }
+        const unsigned bal = g.ballot(act);
+        const int pos = count + __popc(bal & g.lt_mask());
+        if (act && pos < cap) list[pos * stride] = l;
+        count += __popc(bal);
+    }
+    g.sync();
+    return min(count, cap);
+}
+
+// Visit the sphere pairs of a collision term in G-wide batches: every lane of
+// the group calls fn(p) once per batch (p = -1 for a lane without a pair), so
+// ballots inside fn see the whole group.  A term with many sphere pairs per
+// link pair first drops the link pairs whose bounding spheres stay apart.
+template <int G, typename Fn>
+__device__ __forceinline__ void group_for_pairs(const Group<G>& g, const Tabs& t, const Ws& w, const CollEntry& ce,
+                                                Fn fn) {
+    const int* lpoff = t.at<int>(ce.o_lpoff);
+    if (ce.nsp > 32 * ce.nlp) {
+        int* list = reinterpret_cast<int*>(w.raw + ce.ws_slots);
+        const int n = group_broad_phase<G>(g, t, w, ce, list, 1, ce.nlp, false);
+        for (int k = 0; k < n; ++k) {
+            const int l = list[k];
+            const int end = lpoff[l + 1];
+            for (int b0 = lpoff[l]; b0 < end; b0 += G) {
+                const int p = b0 + g.lane;
+                fn(p < end ? p : -1);
+            }
+        }
+    } else {
+        for (int b0 = 0; b0 < ce.nsp; b0 += G) {
+            const int p = b0 + g.lane;
+            fn(p < ce.nsp ? p : -1);
+        }
+    }
+}
+
+// All-pairs terms whose pairs fit 64 G-wide batches keep a per-lane bit mask of
+// active pairs (flat scan); larger terms with many pairs per link pair are pruned.
+template <int G>
+__device__ __forceinline__ bool pairs_by_mask(const CollEntry& ce) {
+    return ce.nsp <= 64 * G && !(ce.nsp > 32 * ce.nlp);
+}
+
+// Penetration of sphere pair `pk` (i | j << 16): margin - surface distance, or
+// a value <= 0 without the square root when the pair is clearly apart.
+__device__ __forceinline__ float pair_penetration(const Ws& w, int pk, float margin) {
+    const float4 a = *reinterpret_cast<const float4*>(w.sph() + 4 * (pk & 0xffff));
+    const float4 b = *reinterpret_cast<const float4*>(w.sph() + 4 * (pk >> 16));
+    const V3 d{a.x - b.x, a.y - b.y, a.z - b.z};
+    const float thr = margin + a.w + b.w;
+    const float d2 = dot(d, d);
+    if (!(thr > 0.f) || d2 >= thr * thr * 1.0001f) return -1.f;
+    return margin - (sqrtf(d2) - a.w - b.w);
 }
 
 // ---------------------------------------------------------------------------
@@ -473,26 +533,26 @@ struct EvalOut {
 };
 
 template <int G>
-__device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
+__device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
     const TabHeader* h = t.h;
     EvalOut o;
     o.Tj = group_fk<G>(g, t, w, q, base);
-    o.S = (o.Tj == w.T0) ? w.T1 : w.T0;
+    o.S = (o.Tj == w.T0()) ? w.T1() : w.T0();
     float* Tj = o.Tj;
     const bool need_sph = h->ncoll > 0;
     if (need_sph) {
         for (int s = g.lane; s < h->ns; s += G) {
-            const Pose P = link_pose(t, Tj, base, t.sphlink[s]);
-            const float* c = t.sph + 4 * s;
+            const Pose P = link_pose(t, Tj, base, t.sphlink()[s]);
+            const float* c = t.sph() + 4 * s;
             const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
-            *reinterpret_cast<float4*>(w.sph + 4 * s) = make_float4(wc.x, wc.y, wc.z, c[3]);
+            *reinterpret_cast<float4*>(w.sph() + 4 * s) = make_float4(wc.x, wc.y, wc.z, c[3]);
         }
-        if (h->max_slots > 0) {
+        {
             for (int l = g.lane; l < h->nl; l += G) {
                 const Pose P = link_pose(t, Tj, base, l);
-                const float* c = t.lbound + 4 * l;
+                const float* c = t.lbound() + 4 * l;
                 const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
-                *reinterpret_cast<float4*>(w.lbw + 4 * l) = make_float4(wc.x, wc.y, wc.z, c[3]);
+                *reinterpret_cast<float4*>(w.lbw() + 4 * l) = make_float4(wc.x, wc.y, wc.z, c[3]);
             }
         }
         g.sync();
@@ -501,9 +561,9 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
     float max_pos = 0.f, max_rot = 0.f;
     // pose entries
     for (int e = g.lane; e < h->npose; e += G) {
-        const PoseEntry& pe = t.pose[e];
+        const PoseEntry& pe = t.pose()[e];
         const Pose P = link_pose(t, Tj, base, pe.link);
-        const float* tg = w.tgt + 8 * e;
+        const float* tg = w.tgt() + 8 * e;
         V3 r;
         if (pe.kind == kPosePosition) {
             const V3 err{tg[0] - P.x, tg[1] - P.y, tg[2] - P.z};
@@ -512,14 +572,14 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
         } else {
             float qw, qi, qj, qk;
             qmul_std(P.w, P.i, P.j, P.k, tg[3], -tg[4], -tg[5], -tg[6], qw, qi, qj, qk);
-            const V3 aa = quat_to_axis_angle(qw, qi, qj, qk);
-            const float sn = fminf(sqrtf(qi * qi + qj * qj + qk * qk), 1.0f);
-            max_rot = fmaxf(max_rot, 2.0f * asinf(sn));
+            float angle;
+            const V3 aa = quat_to_axis_angle(qw, qi, qj, qk, angle);
+            max_rot = fmaxf(max_rot, angle);
             r = V3{pe.w[0] * aa.x, pe.w[1] * aa.y, pe.w[2] * aa.z};
         }
-        w.rpose[3 * e] = r.x;
-        w.rpose[3 * e + 1] = r.y;
-        w.rpose[3 * e + 2] = r.z;
+        w.rpose()[3 * e] = r.x;
+        w.rpose()[3 * e + 1] = r.y;
+        w.rpose()[3 * e + 2] = r.z;
         kadd(ks, kc, r.x * r.x);
         kadd(ks, kc, r.y * r.y);
         kadd(ks, kc, r.z * r.z);
@@ -528,53 +588,52 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
     if (h->has_limit) {
         for (int a = g.lane; a < h->na; a += G) {
             const float v = q[a];
-            const float lo = t.lim[2 * a], hi = t.lim[2 * a + 1];
+            const float lo = t.lim()[2 * a], hi = t.lim()[2 * a + 1];
             const float err = fmaxf(0.f, v - hi) + fmaxf(0.f, lo - v);
-            const float r = t.limw[a] * err;
-            w.rlim[a] = r;
+            const float r = t.limw()[a] * err;
+            w.rlim()[a] = r;
             kadd(ks, kc, r * r);
         }
     }
     // self collision, self_collision_task.py:73-256
     o.nslots = 0;
     for (int ci = 0; ci < h->ncoll; ++ci) {
-        const CollEntry& ce = t.coll[ci];
+        const CollEntry& ce = t.coll()[ci];
         const int* spk = t.at<int>(ce.o_sp);
+        const int* lpoff = t.at<int>(ce.o_lpoff);
         if (ce.mode == 1) {
-            for (int p = g.lane; p < ce.nsp; p += G) {
-                const int pk = spk[p];
-                const int si = pk & 0xffff, sj = pk >> 16;
-                const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * si);
-                const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * sj);
-                const float d = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z});
-                const float pen = ce.margin - (d - a.w - b.w);
-                if (pen > 0.f) {
-                    const float r = ce.weight * pen;
-                    kadd(ks, kc, r * r);
+            if (pairs_by_mask<G>(ce)) {
+                // flat scan; each lane records which of its pairs are active (one bit per
+                // G-wide batch) so the linearisation of this point needs no rescan
+                unsigned long long amask = 0ull;
+                int bit = 0;
+                for (int b0 = 0; b0 < ce.nsp; b0 += G, ++bit) {
+                    const int p = b0 + g.lane;
+                    if (p < ce.nsp) {
+                        const float pen = pair_penetration(w, spk[p], ce.margin);
+                        if (pen > 0.f) {
+                            const float r = ce.weight * pen;
+                            kadd(ks, kc, r * r);
+                            amask |= 1ull << bit;
+                        }
+                    }
                 }
+                reinterpret_cast<unsigned long long*>(w.raw + ce.ws_slots)[g.lane] = amask;
+            } else {
+                group_for_pairs<G>(g, t, w, ce, [&](int p) {
+                    if (p >= 0) {
+                        const float pen = pair_penetration(w, spk[p], ce.margin);
+                        if (pen > 0.f) {
+                            const float r = ce.weight * pen;
+                            kadd(ks, kc, r * r);
+                        }
+                    }
+                });
             }
         } else {
-            const int* lp = t.at<int>(ce.o_lp);
-            const int* lpoff = t.at<int>(ce.o_lpoff);
             Slot* slots = reinterpret_cast<Slot*>(w.raw + ce.ws_slots);
-            int count = 0;
-            // broad phase in link-pair order; the first K penetrating link pairs take the slots
-            for (int b0 = 0; b0 < ce.nlp; b0 += G) {
-                const int l = b0 + g.lane;
-                bool act = false;
-                if (l < ce.nlp) {
-                    const float4 a = *reinterpret_cast<const float4*>(w.lbw + 4 * lp[2 * l]);
-                    const float4 b = *reinterpret_cast<const float4*>(w.lbw + 4 * lp[2 * l + 1]);
-                    const float d = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z});
-                    act = (a.w + b.w + ce.margin - d) > 0.f;
-                }
-                const unsigned bal = g.ballot(act);
-                const int pos = count + __popc(bal & g.lt_mask());
-                if (act && pos < ce.K) slots[pos].lp = l;
-                count += __popc(bal);
-            }
-            const int nsl = min(count, ce.K);
-            g.sync();
+            // the first K penetrating link pairs in link-pair order take the slots
+            const int nsl = group_broad_phase<G>(g, t, w, ce, &slots[0].lp, 4, ce.K, true);
             // narrow phase: first strict minimum of the surface distance per kept link pair
             for (int k = g.lane; k < nsl; k += G) {
                 const int l = slots[k].lp;
@@ -582,8 +641,8 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
                 int bp = lpoff[l];
                 for (int p = lpoff[l]; p < lpoff[l + 1]; ++p) {
                     const int pk = spk[p];
-                    const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * (pk & 0xffff));
-                    const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * (pk >> 16));
+                    const float4 a = *reinterpret_cast<const float4*>(w.sph() + 4 * (pk & 0xffff));
+                    const float4 b = *reinterpret_cast<const float4*>(w.sph() + 4 * (pk >> 16));
                     const float s = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z}) - a.w - b.w;
                     if (s < best) {
                         best = s;
@@ -592,8 +651,8 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
                 }
                 const int pk = spk[bp];
                 const int si = pk & 0xffff, sj = pk >> 16;
-                const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * si);
-                const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * sj);
+                const float4 a = *reinterpret_cast<const float4*>(w.sph() + 4 * si);
+                const float4 b = *reinterpret_cast<const float4*>(w.sph() + 4 * sj);
                 const float surf = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z}) - a.w - b.w;
                 const float r = ce.weight * fmaxf(0.f, ce.margin - surf);
                 slots[k].i = si;
@@ -601,7 +660,7 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
                 slots[k].r = r;
                 kadd(ks, kc, r * r);
             }
-            reinterpret_cast<int*>(w.misc)[8 + ci] = nsl;
+            reinterpret_cast<int*>(w.misc())[8 + ci] = nsl;
             o.nslots += nsl;
         }
     }
@@ -617,45 +676,45 @@ __device__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const flo
 // chunks, compensated J^T J / J^T r accumulation, joint-limit diagonal and the
 // active-DOF mask (lm_optimizer.py:145-189, 872-880; position_task.py:216-272;
 // rotation_task.py:353-401; position_limit.py:538-573;
-// self_collision_task.py:325-385).  Result: w.Hs[0:T] packed lower J^T J,
-// w.Hs[T:T+D] J^T r.
+// self_collision_task.py:325-385).  Result: w.Hs()[0:T] packed lower J^T J,
+// w.Hs()[T:T+D] J^T r.
 // ---------------------------------------------------------------------------
 template <int G>
-__device__ void group_accumulate_chunk(const Group<G>& g, const Tabs& t, Ws& w, int nrows) {
+__device__ __forceinline__ void group_accumulate_chunk(const Group<G>& g, const Tabs& t, Ws& w, int nrows) {
     const TabHeader* h = t.h;
     const int Dp = h->Dp, T = h->T, E = h->E;
     for (int e = g.lane; e < E; e += G) {
         float s = 0.f;
         if (e < T) {
-            const unsigned ab = t.ab[e];
+            const unsigned ab = t.ab()[e];
             const int a = ab >> 8, b = ab & 0xff;
-            const float* ja = w.Jc + a;
-            const float* jb = w.Jc + b;
+            const float* ja = w.Jc() + a;
+            const float* jb = w.Jc() + b;
             for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], jb[r * Dp], s);
         } else {
-            const float* ja = w.Jc + (e - T);
-            for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], w.rc[r], s);
+            const float* ja = w.Jc() + (e - T);
+            for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], w.rc()[r], s);
         }
-        float hs = w.Hs[e], hc = w.Hc[e];
+        float hs = w.Hs()[e], hc = w.Hc()[e];
         kadd(hs, hc, s);
-        w.Hs[e] = hs;
-        w.Hc[e] = hc;
+        w.Hs()[e] = hs;
+        w.Hc()[e] = hc;
     }
     g.sync();
 }
 
 // Build the Jacobian of pose entries [e0, e0+ne) into the chunk (3 rows each).
 template <int G>
-__device__ void group_pose_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* Tj, const float* S,
+__device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* Tj, const float* S,
                                 const float* base, int e0, int ne) {
     const int D = t.h->D, Dp = t.h->Dp;
     const int items = ne * D;
     for (int it = g.lane; it < items; it += G) {
         const int el = it / D, c = it - el * D;
-        const PoseEntry& pe = t.pose[e0 + el];
+        const PoseEntry& pe = t.pose()[e0 + el];
         V3 v, om;
         column_twist(t, S, base, c, pe.link, v, om);
-        float* J = w.Jc + (3 * el) * Dp + c;
+        float* J = w.Jc() + (3 * el) * Dp + c;
         if (pe.kind == kPosePosition) {
             const Pose P = link_pose(t, Tj, base, pe.link);
             const V3 pv = v + cross(om, V3{P.x, P.y, P.z});
@@ -668,22 +727,22 @@ __device__ void group_pose_rows(const Group<G>& g, const Tabs& t, Ws& w, const f
             J[2 * Dp] = pe.w[2] * om.z;
         }
     }
-    for (int r = g.lane; r < 3 * ne; r += G) w.rc[r] = w.rpose[3 * e0 + r];
+    for (int r = g.lane; r < 3 * ne; r += G) w.rc()[r] = w.rpose()[3 * e0 + r];
     g.sync();
 }
 
 // Build collision rows from rowmeta (i, j, residual) records into the chunk.
 template <int G>
-__device__ void group_collision_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* S, const float* base,
+__device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* S, const float* base,
                                      const CollEntry& ce, int nrows) {
     const int D = t.h->D, Dp = t.h->Dp;
     const int items = nrows * D;
     for (int it = g.lane; it < items; it += G) {
         const int r = it / D, c = it - r * D;
-        const float* m = w.rowmeta + 8 * r;
+        const float* m = w.rowmeta() + 4 * r;
         const int si = __float_as_int(m[0]), sj = __float_as_int(m[1]);
-        const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * si);
-        const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * sj);
+        const float4 a = *reinterpret_cast<const float4*>(w.sph() + 4 * si);
+        const float4 b = *reinterpret_cast<const float4*>(w.sph() + 4 * sj);
         const V3 ci{a.x, a.y, a.z}, cj{b.x, b.y, b.z};
         const V3 diff = ci - cj;
         const float dist = norm3(diff);
@@ -693,16 +752,16 @@ __device__ void group_collision_rows(const Group<G>& g, const Tabs& t, Ws& w, co
         if (pen > 0.f) {
             const float den = fmaxf(1e-8f, dist);
             const V3 n{diff.x / den, diff.y / den, diff.z / den};
-            val = -ce.weight * collision_column(t, S, base, c, t.sphlink[si], t.sphlink[sj], ci, cj, n);
+            val = -ce.weight * collision_column(t, S, base, c, t.sphlink()[si], t.sphlink()[sj], ci, cj, n);
         }
-        w.Jc[r * Dp + c] = val;
+        w.Jc()[r * Dp + c] = val;
     }
-    for (int r = g.lane; r < nrows; r += G) w.rc[r] = w.rowmeta[8 * r + 2];
+    for (int r = g.lane; r < nrows; r += G) w.rc()[r] = w.rowmeta()[4 * r + 2];
     g.sync();
 }
 
 template <int G>
-__device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const EvalOut& ev, const float* base) {
+__device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const EvalOut& ev, const float* base) {
     const TabHeader* h = t.h;
     const int D = h->D, T = h->T, E = h->E;
     float* S = ev.S;
@@ -719,8 +778,8 @@ __device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const E
         s[5] = om.z;
     }
     for (int e = g.lane; e < E; e += G) {
-        w.Hs[e] = 0.f;
-        w.Hc[e] = 0.f;
+        w.Hs()[e] = 0.f;
+        w.Hc()[e] = 0.f;
     }
     g.sync();
     // pose rows, kChunkRows/3 entries per chunk
@@ -732,14 +791,14 @@ __device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const E
     }
     // collision rows
     for (int ci = 0; ci < h->ncoll; ++ci) {
-        const CollEntry& ce = t.coll[ci];
+        const CollEntry& ce = t.coll()[ci];
         if (ce.mode == 0) {
             const Slot* slots = reinterpret_cast<const Slot*>(w.raw + ce.ws_slots);
-            const int nsl = reinterpret_cast<const int*>(w.misc)[8 + ci];
+            const int nsl = reinterpret_cast<const int*>(w.misc())[8 + ci];
             for (int k0 = 0; k0 < nsl; k0 += kChunkRows) {
                 const int nr = min(kChunkRows, nsl - k0);
                 for (int r = g.lane; r < nr; r += G) {
-                    float* m = w.rowmeta + 8 * r;
+                    float* m = w.rowmeta() + 4 * r;
                     m[0] = __int_as_float(slots[k0 + r].i);
                     m[1] = __int_as_float(slots[k0 + r].j);
                     m[2] = slots[k0 + r].r;
@@ -750,35 +809,68 @@ __device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const E
             }
         } else {
             const int* spk = t.at<int>(ce.o_sp);
-            int filled = 0;
-            for (int b0 = 0; b0 < ce.nsp; b0 += G) {
-                const int p = b0 + g.lane;
-                bool act = false;
-                float r = 0.f;
-                int pk = 0;
-                if (p < ce.nsp) {
-                    pk = spk[p];
-                    const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * (pk & 0xffff));
-                    const float4 b = *reinterpret_cast<const float4*>(w.sph + 4 * (pk >> 16));
-                    const float d = norm3(V3{a.x - b.x, a.y - b.y, a.z - b.z});
-                    const float pen = ce.margin - (d - a.w - b.w);
-                    act = pen > 0.f;
-                    r = ce.weight * pen;
+            int total = kChunkRows + 1;
+            unsigned long long amask = 0ull;
+            int off = 0;
+            if (pairs_by_mask<G>(ce)) {
+                // rows from the evaluation's activity masks: exclusive scan of the lane counts
+                amask = reinterpret_cast<const unsigned long long*>(w.raw + ce.ws_slots)[g.lane];
+                const int cnt = __popcll(amask);
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < G; o <<= 1) {
+                    const int v = __shfl_up_sync(g.mask, incl, o, G);
+                    if (g.lane >= o) incl += v;
                 }
-                const unsigned bal = g.ballot(act);
-                if (act) {
-                    float* m = w.rowmeta + 8 * (filled + __popc(bal & g.lt_mask()));
+                total = __shfl_sync(g.mask, incl, G - 1, G);
+                off = incl - cnt;
+            }
+            if (total <= kChunkRows) {
+                while (amask) {
+                    const int bit = __ffsll((long long)amask) - 1;
+                    amask &= amask - 1ull;
+                    const int pk = spk[bit * G + g.lane];
+                    float* m = w.rowmeta() + 4 * off++;
                     m[0] = __int_as_float(pk & 0xffff);
                     m[1] = __int_as_float(pk >> 16);
-                    m[2] = r;
+                    m[2] = ce.weight * pair_penetration(w, pk, ce.margin);
                 }
-                filled += __popc(bal);
-                const bool last = b0 + G >= ce.nsp;
-                if (filled > kChunkRows - G || (last && filled > 0)) {
+                g.sync();
+                if (total > 0) {
+                    group_collision_rows<G>(g, t, w, S, base, ce, total);
+                    group_accumulate_chunk<G>(g, t, w, total);
+                }
+            } else {
+                int filled = 0;
+                group_for_pairs<G>(g, t, w, ce, [&](int p) {
+                    bool act = false;
+                    float r = 0.f;
+                    int pk = 0;
+                    if (p >= 0) {
+                        pk = spk[p];
+                        const float pen = pair_penetration(w, pk, ce.margin);
+                        act = pen > 0.f;
+                        r = ce.weight * pen;
+                    }
+                    const unsigned bal = g.ballot(act);
+                    if (act) {
+                        float* m = w.rowmeta() + 4 * (filled + __popc(bal & g.lt_mask()));
+                        m[0] = __int_as_float(pk & 0xffff);
+                        m[1] = __int_as_float(pk >> 16);
+                        m[2] = r;
+                    }
+                    filled += __popc(bal);
+                    if (filled > kChunkRows - G) {
+                        g.sync();
+                        group_collision_rows<G>(g, t, w, S, base, ce, filled);
+                        group_accumulate_chunk<G>(g, t, w, filled);
+                        filled = 0;
+                    }
+                });
+                if (filled > 0) {
                     g.sync();
                     group_collision_rows<G>(g, t, w, S, base, ce, filled);
                     group_accumulate_chunk<G>(g, t, w, filled);
-                    filled = 0;
                 }
             }
         }
@@ -786,18 +878,18 @@ __device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const E
     // finalise: fold compensation, joint-limit diagonal, active-DOF mask
     const int boff = h->base_off;
     for (int e = g.lane; e < E; e += G) {
-        float v = w.Hs[e] + w.Hc[e];
+        float v = w.Hs()[e] + w.Hc()[e];
         int a, b;
         if (e < T) {
-            const unsigned ab = t.ab[e];
+            const unsigned ab = t.ab()[e];
             a = ab >> 8;
             b = ab & 0xff;
             if (h->has_limit && a == b && a >= boff) {
                 const int k = a - boff;
                 const float qv = w.q[k];
-                const float lo = t.lim[2 * k], hi = t.lim[2 * k + 1];
+                const float lo = t.lim()[2 * k], hi = t.lim()[2 * k + 1];
                 const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
-                const float js = t.limw[k] * sg;
+                const float js = t.limw()[k] * sg;
                 v += js * js;
             }
         } else {
@@ -806,13 +898,13 @@ __device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const E
             if (h->has_limit && a >= boff) {
                 const int k = a - boff;
                 const float qv = w.q[k];
-                const float lo = t.lim[2 * k], hi = t.lim[2 * k + 1];
+                const float lo = t.lim()[2 * k], hi = t.lim()[2 * k + 1];
                 const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
-                v += t.limw[k] * sg * w.rlim[k];
+                v += t.limw()[k] * sg * w.rlim()[k];
             }
         }
-        if (h->mask_any) v *= (e < T) ? t.mask[a] * t.mask[b] : t.mask[a];
-        w.Hs[e] = v;
+        if (h->mask_any) v *= (e < T) ? t.mask()[a] * t.mask()[b] : t.mask()[a];
+        w.Hs()[e] = v;
     }
     g.sync();
 }
@@ -820,25 +912,118 @@ __device__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const E
 // ---------------------------------------------------------------------------
 // damped FP64 Cholesky solve (lm_optimizer.py:56-79 / 145-189):
 //   (H + lambda I) delta = -g,  pred = 0.5 delta . (lambda delta - g)
-// H packed lower in `Hp` (fp32), g in Hp[T:].  Step in w.y (fp64) and w.d32.
+// H packed lower in `Hp` (fp32), g in Hp[T:].  Step in w.y() (fp64) and w.d32().
 // Returns false when a pivot is not positive (delta = 0, pred = 0).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int tri(int i, int j) { return (i * (i + 1)) / 2 + j; }
 
+constexpr int kSmallD = 8;  // systems up to this size are factorised in registers
+
+__host__ __device__ constexpr int ctri(int i, int j) { return (i * (i + 1)) / 2 + j; }
+
+// D <= kSmallD: every lane factorises the (identity-padded) system in FP64
+// registers — left-looking Cholesky, forward and back substitution fully
+// unrolled — so the solve needs no shared memory and no synchronisation; all
+// lanes hold the same step.
+// compile-time loop: f(std::integral_constant<int, I>) for I = 0..N-1
+template <typename F, int... I>
+__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void sfor(F&& f) {
+    sfor_impl(f, std::make_integer_sequence<int, N>{});
+}
+
 template <int G>
-__device__ bool group_damped_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
+__device__ __forceinline__ bool group_small_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
+                                  double& pred, double& dnorm) {
+    const int D = t.h->D, T = t.h->T;
+    const double lam = (double)lambda_f;
+    double a[ctri(kSmallD, 0)];
+    double y[kSmallD];
+    sfor<kSmallD>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        sfor<i + 1>([&](auto J) {
+            constexpr int j = decltype(J)::value;
+            double v = (i == j) ? 1.0 : 0.0;
+            if (i < D) v = (double)Hp[ctri(i, j)] + ((i == j) ? lam : 0.0);
+            a[ctri(i, j)] = v;
+        });
+        y[i] = (i < D) ? -(double)Hp[T + i] : 0.0;
+    });
+    bool ok = true;
+    sfor<kSmallD>([&](auto K) {
+        constexpr int k = decltype(K)::value;
+        double s = a[ctri(k, k)];
+        sfor<k>([&](auto M) { constexpr int m = decltype(M)::value; s -= a[ctri(k, m)] * a[ctri(k, m)]; });
+        ok = ok && (s > 0.0);
+        const double inv = rsqrt(s);
+        a[ctri(k, k)] = inv;
+        sfor<kSmallD - k - 1>([&](auto I0) {
+            constexpr int i = k + 1 + decltype(I0)::value;
+            double v = a[ctri(i, k)];
+            sfor<k>([&](auto M) { constexpr int m = decltype(M)::value; v -= a[ctri(i, m)] * a[ctri(k, m)]; });
+            a[ctri(i, k)] = v * inv;
+        });
+    });
+    if (!ok) {
+        for (int i = g.lane; i < D; i += G) w.d32()[i] = 0.f;
+        pred = 0.0;
+        dnorm = 0.0;
+        g.sync();
+        return false;
+    }
+    sfor<kSmallD>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        double v = y[i];
+        sfor<i>([&](auto M) { constexpr int m = decltype(M)::value; v -= a[ctri(i, m)] * y[m]; });
+        y[i] = v * a[ctri(i, i)];
+    });
+    sfor<kSmallD>([&](auto I0) {
+        constexpr int i = kSmallD - 1 - decltype(I0)::value;
+        double v = y[i];
+        sfor<kSmallD - 1 - i>([&](auto M0) {
+            constexpr int m = i + 1 + decltype(M0)::value;
+            v -= a[ctri(m, i)] * y[m];
+        });
+        y[i] = v * a[ctri(i, i)];
+    });
+    double pp = 0.0, nn = 0.0;
+    sfor<kSmallD>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if (i < D) {
+            pp += y[i] * (lam * y[i] - (double)Hp[T + i]);
+            nn += y[i] * y[i];
+        }
+    });
+    pred = 0.5 * pp;
+    dnorm = sqrt(nn);
+    sfor<kSmallD>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if (i < D && (i % G) == g.lane) w.d32()[i] = (float)y[i];
+    });
+    g.sync();
+    return true;
+}
+
+template <int G>
+__device__ __forceinline__ bool group_damped_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
                                    double& pred, double& dnorm) {
     const int D = t.h->D, T = t.h->T;
-    double* L = w.L;
+    if (D <= kSmallD) return group_small_solve<G>(g, t, w, Hp, lambda_f, pred, dnorm);
+    double* L = w.L();
     const double lam = (double)lambda_f;
     for (int e = g.lane; e < T; e += G) {
-        const unsigned ab = t.ab[e];
+        const unsigned ab = t.ab()[e];
         double v = (double)Hp[e];
         if ((ab >> 8) == (ab & 0xff)) v += lam;
         L[e] = v;
     }
-    for (int i = g.lane; i < D; i += G) w.y[i] = -(double)Hp[T + i];
+    for (int i = g.lane; i < D; i += G) w.y()[i] = -(double)Hp[T + i];
     g.sync();
+    // Right-looking factorisation; the diagonal is stored as 1/L_kk so both
+    // triangular solves multiply instead of divide.
     bool ok = true;
     for (int k = 0; k < D; ++k) {
         const double akk = L[tri(k, k)];
@@ -846,68 +1031,57 @@ __device__ bool group_damped_solve(const Group<G>& g, const Tabs& t, Ws& w, cons
             ok = false;
             break;
         }
-        const double d = sqrt(akk);
-        const double inv = 1.0 / d;
+        const double inv = rsqrt(akk);
         g.sync();
         for (int i = k + 1 + g.lane; i < D; i += G) {
             const double l = L[tri(i, k)] * inv;
             L[tri(i, k)] = l;
-            w.tmp[i] = l;
+            w.tmp()[i] = l;
         }
-        if (g.lane == 0) L[tri(k, k)] = d;
+        if (g.lane == 0) L[tri(k, k)] = inv;
         g.sync();
-        // trailing update over the (i, j) items k < j <= i, strided by lane
-        const int m = D - k - 1;
-        int i = k + 1, jj = k + 1 + g.lane;  // row i, column jj
-        while (i < D && jj > i) {
-            jj -= (i - k);
-            ++i;
+        // trailing update: each lane owns rows i = k+1+lane (mod G) and sweeps the
+        // contiguous packed row L[i][k+1..i] (independent updates, unrollable)
+        for (int i = k + 1 + g.lane; i < D; i += G) {
+            const double li = w.tmp()[i];
+            double* row = L + tri(i, 0);
+#pragma unroll 4
+            for (int j = k + 1; j <= i; ++j) row[j] -= li * w.tmp()[j];
         }
-        while (i < D) {
-            L[tri(i, jj)] -= w.tmp[i] * w.tmp[jj];
-            jj += G;
-            while (i < D && jj > i) {
-                jj -= (i - k);
-                ++i;
-            }
-        }
-        (void)m;
         g.sync();
     }
     if (!ok) {
         g.sync();
         for (int i = g.lane; i < D; i += G) {
-            w.y[i] = 0.0;
-            w.d32[i] = 0.f;
+            w.y()[i] = 0.0;
+            w.d32()[i] = 0.f;
         }
         pred = 0.0;
         dnorm = 0.0;
         g.sync();
         return false;
     }
-    // forward substitution L z = -g
+    // forward substitution L z = -g (z into tmp; y[i] for i > k accumulates updates)
     for (int k = 0; k < D; ++k) {
-        const double zk = w.y[k] / L[tri(k, k)];
-        g.sync();
-        if (g.lane == 0) w.y[k] = zk;
-        for (int i = k + 1 + g.lane; i < D; i += G) w.y[i] -= L[tri(i, k)] * zk;
+        const double zk = w.y()[k] * L[tri(k, k)];
+        if (g.lane == 0) w.tmp()[k] = zk;
+        for (int i = k + 1 + g.lane; i < D; i += G) w.y()[i] -= L[tri(i, k)] * zk;
         g.sync();
     }
-    // back substitution L^T x = z
+    // back substitution L^T x = z (x into y; tmp[i] for i < k accumulates updates)
     for (int k = D - 1; k >= 0; --k) {
-        const double xk = w.y[k] / L[tri(k, k)];
-        g.sync();
-        if (g.lane == 0) w.y[k] = xk;
-        for (int i = g.lane; i < k; i += G) w.y[i] -= L[tri(k, i)] * xk;
+        const double xk = w.tmp()[k] * L[tri(k, k)];
+        if (g.lane == 0) w.y()[k] = xk;
+        for (int i = g.lane; i < k; i += G) w.tmp()[i] -= L[tri(k, i)] * xk;
         g.sync();
     }
     double pp = 0.0, nn = 0.0;
     for (int i = g.lane; i < D; i += G) {
-        const double x = w.y[i];
+        const double x = w.y()[i];
         const double gi = (double)Hp[T + i];
         pp += x * (lam * x - gi);
         nn += x * x;
-        w.d32[i] = (float)x;
+        w.d32()[i] = (float)x;
     }
     pred = 0.5 * g.sumd(pp);
     dnorm = sqrt(g.sumd(nn));
@@ -919,25 +1093,25 @@ __device__ bool group_damped_solve(const Group<G>& g, const Tabs& t, Ws& w, cons
 // integrate, robo/robot_kernels.py:563-644 (q + mask * delta; base * exp(delta_base))
 // ---------------------------------------------------------------------------
 template <int G>
-__device__ void group_integrate(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base, float* qo,
+__device__ __forceinline__ void group_integrate(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base, float* qo,
                                 float* baseo) {
     const TabHeader* h = t.h;
     const int boff = h->base_off;
     for (int a = g.lane; a < h->na; a += G) {
-        const float m = h->mask_any ? t.mask[boff + a] : 1.f;
-        qo[a] = q[a] + m * w.d32[boff + a];
+        const float m = h->mask_any ? t.mask()[boff + a] : 1.f;
+        qo[a] = q[a] + m * w.d32()[boff + a];
     }
     if (boff && g.lane == 0) {
         float xi[6];
-        for (int k = 0; k < 6; ++k) xi[k] = w.d32[k];
+        for (int k = 0; k < 6; ++k) xi[k] = w.d32()[k];
         if (h->mask_any)
-            for (int k = 3; k < 6; ++k) xi[k] *= t.mask[k];
+            for (int k = 3; k < 6; ++k) xi[k] *= t.mask()[k];
         const Pose B = pose_load(base);
         Pose N = compose(B, se3_exp(xi, 1e-4f));
         if (h->mask_any) {
-            if (t.mask[0] == 0.f) N.x = B.x;
-            if (t.mask[1] == 0.f) N.y = B.y;
-            if (t.mask[2] == 0.f) N.z = B.z;
+            if (t.mask()[0] == 0.f) N.x = B.x;
+            if (t.mask()[1] == 0.f) N.y = B.y;
+            if (t.mask()[2] == 0.f) N.z = B.z;
         }
         pose_store(baseo, N);
     }

@@ -46,12 +46,12 @@ __device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, W
     const int items = h->npose * 7;
     for (int it = g.lane; it < items; it += G) {
         const int e = it / 7, c = it - 7 * e;
-        const PoseEntry& pe = t.pose[e];
+        const PoseEntry& pe = t.pose()[e];
         const int rows = pe.target_rows > 0 ? pe.target_rows : batch;
         int rep = batch / rows;
         if (rep < 1) rep = 1;
         const int row = min(p / rep, rows - 1);
-        w.tgt[8 * e + c] = pe.targets[((size_t)row * pe.num_frames + pe.frame) * 7 + c];
+        w.tgt()[8 * e + c] = pe.targets[((size_t)row * pe.num_frames + pe.frame) * 7 + c];
     }
 }
 
@@ -71,7 +71,7 @@ __device__ __forceinline__ bool check_stop(LmState& st, const IkLmParams& P) {
 
 // Start a solve at the loaded point: evaluate, linearise, set damping.
 template <int G>
-__device__ void group_start(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P) {
+__device__ __forceinline__ void group_start(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P) {
     const EvalOut ev = group_eval<G>(g, t, w, w.q, cur_base<G>(t, w));
     st.cost = ev.cost;
     st.pos_err = ev.max_pos;
@@ -91,10 +91,10 @@ struct StepTrace {  // optional per-step outputs (ik_step)
 // One LM iteration from the cached linearisation (LMOptimizer._step_body,
 // lm_optimizer.py:834-1005).  Returns true when the problem stops.
 template <int G>
-__device__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
+__device__ __forceinline__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
                               StepTrace* trace = nullptr) {
     double pred = 0.0, dnorm = 0.0;
-    const bool ok = group_damped_solve<G>(g, t, w, w.Hs, st.lambda, pred, dnorm);
+    const bool ok = group_damped_solve<G>(g, t, w, w.Hs(), st.lambda, pred, dnorm);
     if (!ok) st.status |= IK_ST_NOT_SPD;
     if ((P.stop_rules & IK_STOP_STEP) && ok && dnorm < (double)P.step_tol && trace == nullptr) {
         st.status |= IK_ST_CONVERGED;
@@ -141,7 +141,7 @@ __device__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& 
 }
 
 template <int G>
-__device__ void store_solution(const Group<G>& g, const Tabs& t, const Ws& w, const LmState& st, int p, float* q,
+__device__ __forceinline__ void store_solution(const Group<G>& g, const Tabs& t, const Ws& w, const LmState& st, int p, float* q,
                                float* base, float* cost, float* lambda, int* iters, int* status) {
     const TabHeader* h = t.h;
     for (int a = g.lane; a < h->na; a += G) q[(size_t)p * h->na + a] = w.q[a];
@@ -161,7 +161,7 @@ __device__ void store_solution(const Group<G>& g, const Tabs& t, const Ws& w, co
 // sticky stop flag of the all-problems cost rule (opt/optimizer.py:237-239).
 // ---------------------------------------------------------------------------
 template <int G>
-__global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __restrict__ blob, int batch, float* q,
+__global__ void __launch_bounds__(kBlockThreads, 4) lm_plain_kernel(const char* __restrict__ blob, int batch, float* q,
                                                                 float* base, float* rec, IkLmParams P, int mode,
                                                                 int k, int* counters, float* out_cost,
                                                                 float* out_lambda, int* out_iters, int* out_status) {
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __r
             const bool done = (st.status & (IK_ST_CONVERGED | IK_ST_MAX_ITER | IK_ST_NONFINITE)) != 0;
             touched = !done;
             if (!done) {
-                for (int e = g.lane; e < h->E; e += G) w.Hs[e] = r[e];
+                for (int e = g.lane; e < h->E; e += G) w.Hs()[e] = r[e];
                 g.sync();
                 group_iterate<G>(g, t, w, st, P);
                 // the all-problems rule decides the iteration count; without it the cap is max_iter
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __r
         if (all_rule && g.lane == 0 && mode == 1 && !(st.cost <= P.cost_tol)) atomicAdd(&counters[k % 3], 1);
         g.sync();
         if (touched)
-            for (int e = g.lane; e < h->E; e += G) r[e] = w.Hs[e];
+            for (int e = g.lane; e < h->E; e += G) r[e] = w.Hs()[e];
         if (g.lane == 0) {
             RecScalars s;
             s.cost = st.cost;
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(kBlockThreads) lm_plain_kernel(const char* __r
 // each to its own stop rule inside the launch.
 // ---------------------------------------------------------------------------
 template <int G>
-__global__ void __launch_bounds__(kBlockThreads) lm_persistent_kernel(const char* __restrict__ blob, int batch,
+__global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const char* __restrict__ blob, int batch,
                                                                      float* q, float* base, IkLmParams P,
                                                                      int* queue, float* out_cost, float* out_lambda,
                                                                      int* out_iters, int* out_status) {
@@ -256,21 +256,35 @@ __global__ void __launch_bounds__(kBlockThreads) lm_persistent_kernel(const char
     Ws w;
     const int gib = threadIdx.x / G;
     w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    // A warp claims one problem per group at once and its groups iterate in
+    // lockstep until all of them stop: groups that drift out of phase would
+    // make the warp issue each group's instruction stream separately.
+    constexpr int kGroupsPerWarp = 32 / G;
+    const int wg = (threadIdx.x & 31) / G;
     while (true) {
-        int p = 0;
-        if (g.lane == 0) p = atomicAdd(queue, 1);
-        p = g.bcast(p, 0);
-        if (p >= batch) break;
-        load_point<G>(g, t, w, p, q, base);
-        load_targets<G>(g, t, w, p, batch);
-        g.sync();
+        int first = 0;
+        if ((threadIdx.x & 31) == 0) first = atomicAdd(queue, kGroupsPerWarp);
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (first >= batch) break;
+        const int p = first + wg;
+        const bool have = p < batch;
         LmState st;
-        group_start<G>(g, t, w, st, P);
-        bool stop = (st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0;
-        while (!stop) stop = group_iterate<G>(g, t, w, st, P);
-        if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
-        store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
-        g.sync();
+        bool stop = true;
+        if (have) {
+            load_point<G>(g, t, w, p, q, base);
+            load_targets<G>(g, t, w, p, batch);
+            g.sync();
+            group_start<G>(g, t, w, st, P);
+            stop = (st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0;
+        }
+        while (__any_sync(0xffffffffu, !stop)) {
+            if (!stop) stop = group_iterate<G>(g, t, w, st, P);
+        }
+        if (have) {
+            if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
+            store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
+        }
+        __syncwarp();
         // restore the canonical buffer order (the accept path swaps q/qp and base/basep)
         w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
     }
@@ -307,7 +321,7 @@ __global__ void __launch_bounds__(kBlockThreads) fk_kernel(const char* __restric
         if (T_link)
             for (int it = g.lane; it < nl * 7; it += G) {
                 const int l = it / 7, c = it - 7 * l;
-                const int j = t.lpj[l];
+                const int j = t.lpj()[l];
                 float v;
                 if (j >= 0)
                     v = Tj[8 * j + c];
@@ -329,8 +343,8 @@ __global__ void __launch_bounds__(kBlockThreads) fk_kernel(const char* __restric
             }
         if (spheres)
             for (int s = g.lane; s < ns; s += G) {
-                const Pose P = link_pose(t, Tj, b, t.sphlink[s]);
-                const float* c = t.sph + 4 * s;
+                const Pose P = link_pose(t, Tj, b, t.sphlink()[s]);
+                const float* c = t.sph() + 4 * s;
                 const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
                 float* o = spheres + ((size_t)p * ns + s) * 3;
                 o[0] = wc.x;
@@ -340,7 +354,7 @@ __global__ void __launch_bounds__(kBlockThreads) fk_kernel(const char* __restric
         if (link_bounds)
             for (int l = g.lane; l < nl; l += G) {
                 const Pose P = link_pose(t, Tj, b, l);
-                const float* c = t.lbound + 4 * l;
+                const float* c = t.lbound() + 4 * l;
                 const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
                 float* o = link_bounds + ((size_t)p * nl + l) * 3;
                 o[0] = wc.x;
@@ -372,7 +386,7 @@ __global__ void __launch_bounds__(kBlockThreads) link_jacobian_kernel(const char
         g.sync();
         const float* b = cur_base<G>(t, w);
         float* Tj = group_fk<G>(g, t, w, w.q, b);
-        float* S = (Tj == w.T0) ? w.T1 : w.T0;
+        float* S = (Tj == w.T0()) ? w.T1() : w.T0();
         for (int j = g.lane; j < h->nj; j += G) {
             V3 v, om;
             joint_subspace(t, Tj, j, v, om);
@@ -456,9 +470,9 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
         float* Jo = Jout ? Jout + (size_t)p * R * D : nullptr;
         // residuals
         if (ro) {
-            for (int r = g.lane; r < 3 * h->npose; r += G) ro[t.pose[r / 3].out_row + r % 3] = w.rpose[r];
+            for (int r = g.lane; r < 3 * h->npose; r += G) ro[t.pose()[r / 3].out_row + r % 3] = w.rpose()[r];
             if (h->has_limit)
-                for (int a = g.lane; a < h->na; a += G) ro[h->limit_row + a] = w.rlim[a];
+                for (int a = g.lane; a < h->na; a += G) ro[h->limit_row + a] = w.rlim()[a];
         }
         float* S = ev.S;
         for (int j = g.lane; j < h->nj; j += G) {
@@ -480,31 +494,31 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 group_pose_rows<G>(g, t, w, ev.Tj, S, b, e0, ne);
                 for (int it = g.lane; it < 3 * ne * D; it += G) {
                     const int rr = it / D, c = it - rr * D;
-                    const int row = t.pose[e0 + rr / 3].out_row + rr % 3;
-                    Jo[(size_t)row * D + c] = w.Jc[rr * Dp + c];
+                    const int row = t.pose()[e0 + rr / 3].out_row + rr % 3;
+                    Jo[(size_t)row * D + c] = w.Jc()[rr * Dp + c];
                 }
                 g.sync();
             }
             if (h->has_limit)
                 for (int a = g.lane; a < h->na; a += G) {
                     const float qv = w.q[a];
-                    const float lo = t.lim[2 * a], hi = t.lim[2 * a + 1];
+                    const float lo = t.lim()[2 * a], hi = t.lim()[2 * a + 1];
                     const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
-                    Jo[(size_t)(h->limit_row + a) * D + boff + a] = t.limw[a] * sg;
+                    Jo[(size_t)(h->limit_row + a) * D + boff + a] = t.limw()[a] * sg;
                 }
         }
         for (int ci = 0; ci < h->ncoll; ++ci) {
-            const CollEntry& ce = t.coll[ci];
+            const CollEntry& ce = t.coll()[ci];
             const int* spk = t.at<int>(ce.o_sp);
             if (ce.mode == 0) {
                 const Slot* slots = reinterpret_cast<const Slot*>(w.raw + ce.ws_slots);
-                const int nsl = reinterpret_cast<const int*>(w.misc)[8 + ci];
+                const int nsl = reinterpret_cast<const int*>(w.misc())[8 + ci];
                 if (ro)
                     for (int k = g.lane; k < nsl; k += G) ro[ce.out_row + k] = slots[k].r;
                 for (int k0 = 0; Jo && k0 < nsl; k0 += kChunkRows) {
                     const int nr = min(kChunkRows, nsl - k0);
                     for (int r = g.lane; r < nr; r += G) {
-                        float* m = w.rowmeta + 8 * r;
+                        float* m = w.rowmeta() + 4 * r;
                         m[0] = __int_as_float(slots[k0 + r].i);
                         m[1] = __int_as_float(slots[k0 + r].j);
                         m[2] = slots[k0 + r].r;
@@ -514,7 +528,7 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                     group_collision_rows<G>(g, t, w, S, b, ce, nr);
                     for (int it = g.lane; it < nr * D; it += G) {
                         const int rr = it / D, c = it - rr * D;
-                        Jo[(size_t)(ce.out_row + k0 + rr) * D + c] = w.Jc[rr * Dp + c];
+                        Jo[(size_t)(ce.out_row + k0 + rr) * D + c] = w.Jc()[rr * Dp + c];
                     }
                     g.sync();
                 }
@@ -523,12 +537,12 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                     const int nr = min(kChunkRows, ce.nsp - p0);
                     for (int r = g.lane; r < nr; r += G) {
                         const int pk = spk[p0 + r];
-                        const float4 a = *reinterpret_cast<const float4*>(w.sph + 4 * (pk & 0xffff));
-                        const float4 bb = *reinterpret_cast<const float4*>(w.sph + 4 * (pk >> 16));
+                        const float4 a = *reinterpret_cast<const float4*>(w.sph() + 4 * (pk & 0xffff));
+                        const float4 bb = *reinterpret_cast<const float4*>(w.sph() + 4 * (pk >> 16));
                         const float d = norm3(V3{a.x - bb.x, a.y - bb.y, a.z - bb.z});
                         const float pen = ce.margin - (d - a.w - bb.w);
                         const float res = ce.weight * fmaxf(0.f, pen);
-                        float* m = w.rowmeta + 8 * r;
+                        float* m = w.rowmeta() + 4 * r;
                         m[0] = __int_as_float(pk & 0xffff);
                         m[1] = __int_as_float(pk >> 16);
                         m[2] = res;
@@ -539,7 +553,7 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                         group_collision_rows<G>(g, t, w, S, b, ce, nr);
                         for (int it = g.lane; it < nr * D; it += G) {
                             const int rr = it / D, c = it - rr * D;
-                            Jo[(size_t)(ce.out_row + p0 + rr) * D + c] = w.Jc[rr * Dp + c];
+                            Jo[(size_t)(ce.out_row + p0 + rr) * D + c] = w.Jc()[rr * Dp + c];
                         }
                     }
                     g.sync();
@@ -575,13 +589,13 @@ __global__ void __launch_bounds__(kBlockThreads) normal_kernel(const char* __res
         group_linearize<G>(g, t, w, ev, b);
         if (H)
             for (int e = g.lane; e < T; e += G) {
-                const unsigned ab = t.ab[e];
+                const unsigned ab = t.ab()[e];
                 const int a = ab >> 8, c = ab & 0xff;
-                H[(size_t)p * D * D + a * D + c] = w.Hs[e];
-                H[(size_t)p * D * D + c * D + a] = w.Hs[e];
+                H[(size_t)p * D * D + a * D + c] = w.Hs()[e];
+                H[(size_t)p * D * D + c * D + a] = w.Hs()[e];
             }
         if (gv)
-            for (int i = g.lane; i < D; i += G) gv[(size_t)p * D + i] = w.Hs[T + i];
+            for (int i = g.lane; i < D; i += G) gv[(size_t)p * D + i] = w.Hs()[T + i];
         if (cost && g.lane == 0) cost[p] = ev.cost;
         g.sync();
     }
@@ -606,14 +620,14 @@ __global__ void __launch_bounds__(kBlockThreads) damped_solve_kernel(const char*
     const int D = h->D, T = h->T;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
         for (int e = g.lane; e < T; e += G) {
-            const unsigned ab = t.ab[e];
-            w.Hs[e] = H[(size_t)p * D * D + (ab >> 8) * D + (ab & 0xff)];
+            const unsigned ab = t.ab()[e];
+            w.Hs()[e] = H[(size_t)p * D * D + (ab >> 8) * D + (ab & 0xff)];
         }
-        for (int i = g.lane; i < D; i += G) w.Hs[T + i] = gv[(size_t)p * D + i];
+        for (int i = g.lane; i < D; i += G) w.Hs()[T + i] = gv[(size_t)p * D + i];
         g.sync();
         double pr = 0.0, dn = 0.0;
-        const bool ok = group_damped_solve<G>(g, t, w, w.Hs, lambda[p], pr, dn);
-        for (int i = g.lane; i < D; i += G) delta[(size_t)p * D + i] = w.d32[i];
+        const bool ok = group_damped_solve<G>(g, t, w, w.Hs(), lambda[p], pr, dn);
+        for (int i = g.lane; i < D; i += G) delta[(size_t)p * D + i] = w.d32()[i];
         if (g.lane == 0) {
             pred[p] = (float)pr;
             if (spd) spd[p] = ok ? 1 : 0;
@@ -651,7 +665,7 @@ __global__ void __launch_bounds__(kBlockThreads) step_kernel(const char* __restr
         StepTrace tr;
         group_iterate<G>(g, t, w, st, P1, &tr);
         if (delta)
-            for (int i = g.lane; i < D; i += G) delta[(size_t)p * D + i] = w.d32[i];
+            for (int i = g.lane; i < D; i += G) delta[(size_t)p * D + i] = w.d32()[i];
         if (g.lane == 0) {
             lambda[p] = st.lambda;
             if (cost) cost[p] = tr.accepted ? tr.cost_new : tr.cost_before;
