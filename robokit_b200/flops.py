@@ -104,11 +104,10 @@ def work_model(spec: Any, term_descs: Sequence[dict], floating: bool, active_col
             nsp = d["num_sphere_pairs"]
             if d["pair_mode"] == 1:
                 ev += PAIR_TEST * nsp
-                lin += PAIR_TEST * nsp  # the linearisation rescans the pairs to compact the active rows
             else:
                 nlp = d["num_link_pairs"]
                 ev += PAIR_TEST * nlp + SPHERE * spec.num_links
-                ev += PAIR_TEST * min(nsp, nsp)  # narrow phase bounded by the pairs of the kept link pairs
+                ev += PAIR_TEST * nsp  # narrow phase: at most every pair of the kept link pairs
             # active rows: normal + per-joint terms over the two links' ancestors
             lin += active_collision_rows * (12 + 34 * max(1, int(np.mean(np.sum(anc, axis=1)))) * 2)
     rows_lin = rows + active_collision_rows
