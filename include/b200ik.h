@@ -177,6 +177,27 @@ int ik_solve_plain(IkProblem* problem, int32_t batch, float* d_q, float* d_base,
 int ik_solve_persistent(IkProblem* problem, int32_t batch, float* d_q, float* d_base, const IkLmParams* params,
                         float* d_cost, float* d_lambda, int32_t* d_iters, int32_t* d_status, void* stream);
 
+/* The persistent solve with no device allocation.  This entry point has no
+ * counterpart in the reference.  It is for callers that may not allocate
+ * device memory once running: a real-time control loop that forbids
+ * allocation after start-up, or a plug-in whose host framework owns every
+ * device buffer.  It takes the robot and term descriptors directly (as
+ * ik_robot_create and ik_problem_create do), lowers them on the host every
+ * call, and keeps the table blob and the work-queue counter in a static
+ * device array of the library (IK_NOALLOC_MAX_TABLE_BYTES for the tables plus
+ * 256 B); the counter is zeroed on `stream` before each launch.  Tables larger
+ * than the limit are refused with IK_E_UNSUPPORTED.
+ * - The first call on a device looks up that array's address (once per
+ *   device, with the device current); make it before any stream capture.
+ * - The array is shared by all calls on a device: calls that overlap in time
+ *   race on it and must be serialised by the caller.
+ * Arguments and outputs are those of ik_problem_create + ik_solve_persistent. */
+#define IK_NOALLOC_MAX_TABLE_BYTES (224 * 1024)
+int ik_solve_persistent_noalloc(const IkRobotDesc* robot, int32_t floating_base, const IkTermDesc* terms,
+                                int32_t num_terms, const float* active_dof_mask, int32_t batch, float* d_q,
+                                float* d_base, const IkLmParams* params, float* d_cost, float* d_lambda,
+                                int32_t* d_iters, int32_t* d_status, void* stream);
+
 /* Pick the lane-group width (8, 16 or 32 lanes per problem; 0 = automatic)
  * and the resident groups per SM of the persistent form (0 = automatic). */
 int ik_problem_set_schedule(IkProblem* problem, int32_t group_lanes, int32_t blocks_per_sm);

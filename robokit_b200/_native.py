@@ -149,6 +149,11 @@ _SIGNATURES = {
         ctypes.c_int,
         [_vp, ctypes.c_int32, _vp, _vp, ctypes.POINTER(IkLmParams), _vp, _vp, _vp, _vp, _vp],
     ),
+    "ik_solve_persistent_noalloc": (
+        ctypes.c_int,
+        [ctypes.POINTER(IkRobotDesc), ctypes.c_int32, ctypes.POINTER(IkTermDesc), ctypes.c_int32, _vp,
+         ctypes.c_int32, _vp, _vp, ctypes.POINTER(IkLmParams), _vp, _vp, _vp, _vp, _vp],
+    ),
     "ik_fk": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ik_link_jacobian": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp]),
     "ik_residual_jacobian": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]),

@@ -46,7 +46,8 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", os.path.join(CSRC, "ik_api.cu"), "-o", OUT + ".tmp"]
+    units = [os.path.join(CSRC, "ik_api.cu"), os.path.join(CSRC, "ik_noalloc.cu")]
+    cmd = [nvcc, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", *units, "-o", OUT + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

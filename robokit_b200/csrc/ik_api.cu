@@ -11,24 +11,18 @@
 #include <vector>
 
 #include "b200ik.h"
+#include "ik_host.h"
 #include "ik_kernels.cuh"
 
 using namespace b200ik;
+using host::ProblemTables;
+using host::RobotHost;
+using host::TermHost;
 
 namespace {
 
 thread_local std::string g_last_error;
 std::atomic<long long> g_launches{0};
-
-int fail(int code, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
-    va_end(ap);
-    g_last_error = buf;
-    return code;
-}
 
 #define CK(call)                                                                           \
     do {                                                                                   \
@@ -37,19 +31,6 @@ int fail(int code, const char* fmt, ...) {
     } while (0)
 
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
-
-// ----------------------------------------------------------------------------
-// host copy of a robot
-// ----------------------------------------------------------------------------
-struct RobotHost {
-    int nj = 0, nl = 0, na = 0, ns = 0;
-    std::vector<int> jtype, jparent, jact, jmimic, lpj, sphlink;
-    std::vector<float> jmul, joff, jaxis, jpt, lim, sph, lbound;
-    std::vector<unsigned long long> lanc;  // per link: ancestor joints
-    std::vector<int> colstart, coljoint;
-    std::vector<float> colmul;
-    int fk_rounds = 0;
-};
 
 struct BlobBuilder {
     std::vector<char> buf;
@@ -66,15 +47,23 @@ struct BlobBuilder {
     TabHeader* hdr() { return reinterpret_cast<TabHeader*>(buf.data()); }
 };
 
-struct TermHost {
-    IkTermDesc d;
-    std::vector<int> frame_links;
-    std::vector<float> weights;
-    std::vector<int> lp, lpoff, sp;
-    int row = 0, rows = 0;
-};
-
 }  // namespace
+
+namespace b200ik {
+namespace host {
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+}  // namespace host
+}  // namespace b200ik
+using host::fail;
 
 struct IkRobot {
     RobotHost h;
@@ -99,7 +88,8 @@ struct IkProblem {
     int blocks_per_sm = 0;  // 0 = automatic
 };
 
-namespace {
+namespace b200ik {
+namespace host {
 
 int num_sms() {
     static int sms = -1;
@@ -228,25 +218,6 @@ int choose_group(int D, int blob_bytes, int ws_bytes, int requested) {
     return G;
 }
 
-template <typename K>
-int prepare_kernel(K kernel, int smem) {
-    if (smem > max_smem_optin()) return fail(IK_E_UNSUPPORTED, "shared memory %d B exceeds the device limit", smem);
-    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    return IK_OK;
-}
-
-template <typename K>
-int grid_for(K kernel, int smem, int batch, int G, int blocks_per_sm_req, int& grid) {
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlockThreads, smem));
-    if (per_sm <= 0) return fail(IK_E_UNSUPPORTED, "kernel does not fit on an SM (smem %d B)", smem);
-    if (blocks_per_sm_req > 0) per_sm = std::min(per_sm, blocks_per_sm_req);
-    const int gpb = kBlockThreads / G;
-    const int need = (batch + gpb - 1) / gpb;
-    grid = std::max(1, std::min(need, per_sm * num_sms()));
-    return IK_OK;
-}
-
 int check_launch() {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(IK_E_CUDA, "kernel launch: %s", cudaGetErrorString(e));
@@ -319,44 +290,14 @@ int validate_robot(const IkRobotDesc* d) {
     return IK_OK;
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace b200ik
+using namespace b200ik::host;
 
 // =============================================================================
-extern "C" {
-
-const char* ik_last_error(void) { return g_last_error.c_str(); }
-int ik_version(void) { return 10000; }
-
-int ik_device_count(int* out) {
-    if (!out) return fail(IK_E_INVALID, "out is NULL");
-    int n = 0;
-    cudaError_t e = cudaGetDeviceCount(&n);
-    if (e != cudaSuccess) {
-        *out = 0;
-        return fail(IK_E_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
-    }
-    *out = n;
-    return IK_OK;
-}
-
-int ik_set_device(int device) {
-    CK(cudaSetDevice(device));
-    return IK_OK;
-}
-
-int ik_launch_count(int64_t* out) {
-    if (!out) return fail(IK_E_INVALID, "out is NULL");
-    *out = g_launches.load();
-    return IK_OK;
-}
-
-int ik_robot_create(const IkRobotDesc* d, IkRobot** out) {
-    if (!out) return fail(IK_E_INVALID, "out is NULL");
-    *out = nullptr;
+int b200ik::host::fill_robot(const IkRobotDesc* d, RobotHost& r) {
     int rc = validate_robot(d);
     if (rc) return rc;
-    IkRobot* R = new IkRobot();
-    RobotHost& r = R->h;
     r.nj = d->num_joints;
     r.nl = d->num_links;
     r.na = d->num_actuated;
@@ -431,6 +372,47 @@ int ik_robot_create(const IkRobotDesc* d, IkRobot** out) {
     int rounds = 0;
     while ((1 << rounds) < maxd) ++rounds;
     r.fk_rounds = rounds;
+    return IK_OK;
+}
+
+extern "C" {
+
+const char* ik_last_error(void) { return g_last_error.c_str(); }
+int ik_version(void) { return 10000; }
+
+int ik_device_count(int* out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *out = 0;
+        return fail(IK_E_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    *out = n;
+    return IK_OK;
+}
+
+int ik_set_device(int device) {
+    CK(cudaSetDevice(device));
+    return IK_OK;
+}
+
+int ik_launch_count(int64_t* out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    *out = g_launches.load();
+    return IK_OK;
+}
+
+int ik_robot_create(const IkRobotDesc* d, IkRobot** out) {
+    if (!out) return fail(IK_E_INVALID, "out is NULL");
+    *out = nullptr;
+    IkRobot* R = new IkRobot();
+    const int rc = fill_robot(d, R->h);
+    if (rc) {
+        delete R;
+        return rc;
+    }
+    RobotHost& r = R->h;
     for (int f = 0; f < 2; ++f) {
         std::vector<char> blob;
         int ws = 0;
@@ -464,26 +446,31 @@ int ik_robot_destroy(IkRobot* robot) {
 
 namespace {
 
-int build_problem_blob(IkProblem* P) {
-    const RobotHost& r = P->robot->h;
+}  // namespace
+
+int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vector<TermHost>& terms,
+                               const std::vector<float>& mask_in, int R, ProblemTables& out) {
     BlobBuilder b;
     add_robot_tables(b, r);
     TabHeader* h = b.hdr();
-    const int boff = P->floating ? 6 : 0;
+    const int boff = floating ? 6 : 0;
     h->D = boff + r.na;
     h->base_off = boff;
     h->T = h->D * (h->D + 1) / 2;
     h->E = h->T + h->D;
     h->Dp = h->D;
-    h->mask_any = P->mask_any;
-    h->R_ref = P->R;
+    int mask_any = 0;
+    for (float m : mask_in)
+        if (m != 1.f) mask_any = 1;
+    h->mask_any = mask_any;
+    h->R_ref = R;
     // pose entries
     std::vector<PoseEntry> pose;
     std::vector<CollEntry> coll;
     std::vector<float> limw(std::max(r.na, 1), 0.f);
     int has_limit = 0, limit_row = 0;
-    for (size_t ti = 0; ti < P->terms.size(); ++ti) {
-        const TermHost& th = P->terms[ti];
+    for (size_t ti = 0; ti < terms.size(); ++ti) {
+        const TermHost& th = terms[ti];
         const int kind = th.d.kind;
         if (kind == IK_TERM_POSITION || kind == IK_TERM_ROTATION) {
             for (int f = 0; f < th.d.num_frames; ++f) {
@@ -513,8 +500,8 @@ int build_problem_blob(IkProblem* P) {
     // collision arrays
     int slot_bytes = 0;
     std::vector<int> coll_slot_rel;
-    for (size_t ti = 0; ti < P->terms.size(); ++ti) {
-        const TermHost& th = P->terms[ti];
+    for (size_t ti = 0; ti < terms.size(); ++ti) {
+        const TermHost& th = terms[ti];
         if (th.d.kind != IK_TERM_SELF_COLLISION) continue;
         CollEntry c;
         std::memset(&c, 0, sizeof(c));
@@ -545,7 +532,7 @@ int build_problem_blob(IkProblem* P) {
     b.hdr()->o_coll = o_coll;
     o = b.addv(limw);
     b.hdr()->o_limw = o;
-    std::vector<float> mask = P->mask;
+    std::vector<float> mask = mask_in;
     if (mask.empty()) mask.assign(b.hdr()->D, 1.f);
     o = b.addv(mask);
     b.hdr()->o_mask = o;
@@ -559,10 +546,111 @@ int build_problem_blob(IkProblem* P) {
     CollEntry* ce = reinterpret_cast<CollEntry*>(b.buf.data() + o_coll);
     for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
     h->bytes = (int)b.buf.size();
-    P->blob = b.buf;
-    P->blob_bytes = h->bytes;
-    P->ws_bytes = h->ws_bytes;
-    P->E = h->E;
+    out.blob = b.buf;
+    out.blob_bytes = h->bytes;
+    out.ws_bytes = h->ws_bytes;
+    out.D = h->D;
+    out.R = R;
+    out.E = h->E;
+    return IK_OK;
+}
+
+int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc* terms, int num_terms,
+                              std::vector<TermHost>& out, int& R) {
+    (void)floating;
+    out.clear();
+    if (num_terms < 0 || (num_terms > 0 && !terms)) return fail(IK_E_INVALID, "terms array is NULL");
+    int row = 0, nlimit = 0;
+    for (int i = 0; i < num_terms; ++i) {
+        const IkTermDesc& d = terms[i];
+        TermHost th;
+        th.d = d;
+        th.row = row;
+        if (d.kind == IK_TERM_POSITION || d.kind == IK_TERM_ROTATION) {
+            if (d.num_frames < 1 || !d.frame_links || !d.weights) {
+                return fail(IK_E_INVALID, "term %d: pose term needs frames and weights", i);
+            }
+            if (!d.d_targets) {
+                return fail(IK_E_INVALID, "term %d: pose term needs a target array", i);
+            }
+            th.frame_links.assign(d.frame_links, d.frame_links + d.num_frames);
+            for (int f : th.frame_links)
+                if (f < 0 || f >= r.nl) {
+                        return fail(IK_E_INVALID, "term %d: frame link %d out of range", i, f);
+                }
+            th.weights.assign(d.weights, d.weights + 3 * d.num_frames);
+            th.rows = 3 * d.num_frames;
+        } else if (d.kind == IK_TERM_POSITION_LIMIT) {
+            if (++nlimit > 1) {
+                return fail(IK_E_UNSUPPORTED, "more than one PositionLimit term");
+            }
+            if (!d.weights && r.na > 0) {
+                return fail(IK_E_INVALID, "term %d: limit weights are NULL", i);
+            }
+            th.weights.assign(d.weights, d.weights + r.na);
+            th.rows = r.na;
+        } else if (d.kind == IK_TERM_SELF_COLLISION) {
+            if (r.ns < 2) {
+                return fail(IK_E_INVALID, "term %d: robot has no collision spheres", i);
+            }
+            if (d.pair_mode != IK_PAIRS_SLOTS && d.pair_mode != IK_PAIRS_ALL) {
+                return fail(IK_E_INVALID, "term %d: pair_mode %d", i, d.pair_mode);
+            }
+            if (d.pair_mode == IK_PAIRS_SLOTS && d.max_active_pairs < 1) {
+                return fail(IK_E_INVALID, "max_active_pairs must be >= 1.");
+            }
+            if (!d.weights) {
+                return fail(IK_E_INVALID, "term %d: weight is NULL", i);
+            }
+            th.weights.assign(d.weights, d.weights + 1);
+            if (d.num_link_pairs < 0 || d.num_sphere_pairs < 0 ||
+                (d.num_link_pairs > 0 && (!d.link_pairs || !d.link_pair_offsets || !d.sphere_pairs))) {
+                return fail(IK_E_INVALID, "term %d: pair tables are inconsistent", i);
+            }
+            th.lp.assign(d.link_pairs, d.link_pairs + 2 * d.num_link_pairs);
+            th.lpoff.assign(d.link_pair_offsets, d.link_pair_offsets + d.num_link_pairs + 1);
+            if (d.num_link_pairs == 0) th.lpoff.assign(1, 0);
+            if (th.lpoff.front() != 0 || th.lpoff.back() != d.num_sphere_pairs) {
+                return fail(IK_E_INVALID, "term %d: link pair offsets do not cover the sphere pairs", i);
+            }
+            for (int k = 0; k < d.num_link_pairs; ++k) {
+                if (th.lpoff[k + 1] < th.lpoff[k]) {
+                        return fail(IK_E_INVALID, "term %d: link pair offsets decrease", i);
+                }
+                for (int s = 0; s < 2; ++s)
+                    if (th.lp[2 * k + s] < 0 || th.lp[2 * k + s] >= r.nl) {
+                                return fail(IK_E_INVALID, "term %d: link pair %d out of range", i, k);
+                    }
+            }
+            th.sp.resize(d.num_sphere_pairs);
+            for (int k = 0; k < d.num_sphere_pairs; ++k) {
+                const int a = d.sphere_pairs[2 * k], b = d.sphere_pairs[2 * k + 1];
+                if (a < 0 || a >= r.ns || b < 0 || b >= r.ns) {
+                        return fail(IK_E_INVALID, "term %d: sphere pair %d out of range", i, k);
+                }
+                th.sp[k] = a | (b << 16);
+            }
+            th.rows = d.pair_mode == IK_PAIRS_SLOTS ? d.max_active_pairs : d.num_sphere_pairs;
+        } else {
+            return fail(IK_E_INVALID, "term %d: unknown kind %d", i, d.kind);
+        }
+        row += th.rows;
+        out.push_back(th);
+    }
+    R = row;
+    return IK_OK;
+}
+
+namespace {
+
+int build_problem_blob(IkProblem* P) {
+    ProblemTables t;
+    const int rc = build_tables(P->robot->h, P->floating, P->terms, P->mask, P->R, t);
+    if (rc) return rc;
+    P->blob = std::move(t.blob);
+    P->blob_bytes = t.blob_bytes;
+    P->ws_bytes = t.ws_bytes;
+    P->E = t.E;
     return IK_OK;
 }
 
@@ -590,7 +678,8 @@ int check_batch(const IkProblem* P, int batch) {
     return IK_OK;
 }
 
-int check_params(const IkLmParams* p) {
+}  // namespace
+int b200ik::host::check_params(const IkLmParams* p) {
     if (!p) return fail(IK_E_INVALID, "params is NULL");
     if (!(p->lambda_factor > 0.f) || !(p->lambda_min >= 0.f) || !(p->lambda_max >= p->lambda_min))
         return fail(IK_E_INVALID, "damping parameters are inconsistent");
@@ -598,6 +687,7 @@ int check_params(const IkLmParams* p) {
     return IK_OK;
 }
 
+namespace {
 }  // namespace
 
 extern "C" {
@@ -618,105 +708,17 @@ int ik_problem_create(IkRobot* robot, int32_t capacity, int32_t floating_base, c
     P->capacity = capacity;
     P->floating = floating_base ? 1 : 0;
     P->D = D;
-    int row = 0, nlimit = 0;
-    for (int i = 0; i < num_terms; ++i) {
-        const IkTermDesc& d = terms[i];
-        TermHost th;
-        th.d = d;
-        th.row = row;
-        if (d.kind == IK_TERM_POSITION || d.kind == IK_TERM_ROTATION) {
-            if (d.num_frames < 1 || !d.frame_links || !d.weights) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: pose term needs frames and weights", i);
-            }
-            if (!d.d_targets) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: pose term needs a target array", i);
-            }
-            th.frame_links.assign(d.frame_links, d.frame_links + d.num_frames);
-            for (int f : th.frame_links)
-                if (f < 0 || f >= r.nl) {
-                    delete P;
-                    return fail(IK_E_INVALID, "term %d: frame link %d out of range", i, f);
-                }
-            th.weights.assign(d.weights, d.weights + 3 * d.num_frames);
-            th.rows = 3 * d.num_frames;
-        } else if (d.kind == IK_TERM_POSITION_LIMIT) {
-            if (++nlimit > 1) {
-                delete P;
-                return fail(IK_E_UNSUPPORTED, "more than one PositionLimit term");
-            }
-            if (!d.weights && r.na > 0) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: limit weights are NULL", i);
-            }
-            th.weights.assign(d.weights, d.weights + r.na);
-            th.rows = r.na;
-        } else if (d.kind == IK_TERM_SELF_COLLISION) {
-            if (r.ns < 2) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: robot has no collision spheres", i);
-            }
-            if (d.pair_mode != IK_PAIRS_SLOTS && d.pair_mode != IK_PAIRS_ALL) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: pair_mode %d", i, d.pair_mode);
-            }
-            if (d.pair_mode == IK_PAIRS_SLOTS && d.max_active_pairs < 1) {
-                delete P;
-                return fail(IK_E_INVALID, "max_active_pairs must be >= 1.");
-            }
-            if (!d.weights) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: weight is NULL", i);
-            }
-            th.weights.assign(d.weights, d.weights + 1);
-            if (d.num_link_pairs < 0 || d.num_sphere_pairs < 0 ||
-                (d.num_link_pairs > 0 && (!d.link_pairs || !d.link_pair_offsets || !d.sphere_pairs))) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: pair tables are inconsistent", i);
-            }
-            th.lp.assign(d.link_pairs, d.link_pairs + 2 * d.num_link_pairs);
-            th.lpoff.assign(d.link_pair_offsets, d.link_pair_offsets + d.num_link_pairs + 1);
-            if (d.num_link_pairs == 0) th.lpoff.assign(1, 0);
-            if (th.lpoff.front() != 0 || th.lpoff.back() != d.num_sphere_pairs) {
-                delete P;
-                return fail(IK_E_INVALID, "term %d: link pair offsets do not cover the sphere pairs", i);
-            }
-            for (int k = 0; k < d.num_link_pairs; ++k) {
-                if (th.lpoff[k + 1] < th.lpoff[k]) {
-                    delete P;
-                    return fail(IK_E_INVALID, "term %d: link pair offsets decrease", i);
-                }
-                for (int s = 0; s < 2; ++s)
-                    if (th.lp[2 * k + s] < 0 || th.lp[2 * k + s] >= r.nl) {
-                        delete P;
-                        return fail(IK_E_INVALID, "term %d: link pair %d out of range", i, k);
-                    }
-            }
-            th.sp.resize(d.num_sphere_pairs);
-            for (int k = 0; k < d.num_sphere_pairs; ++k) {
-                const int a = d.sphere_pairs[2 * k], b = d.sphere_pairs[2 * k + 1];
-                if (a < 0 || a >= r.ns || b < 0 || b >= r.ns) {
-                    delete P;
-                    return fail(IK_E_INVALID, "term %d: sphere pair %d out of range", i, k);
-                }
-                th.sp[k] = a | (b << 16);
-            }
-            th.rows = d.pair_mode == IK_PAIRS_SLOTS ? d.max_active_pairs : d.num_sphere_pairs;
-        } else {
-            delete P;
-            return fail(IK_E_INVALID, "term %d: unknown kind %d", i, d.kind);
-        }
-        row += th.rows;
-        P->terms.push_back(th);
+    int rc = fill_terms(r, P->floating, terms, num_terms, P->terms, P->R);
+    if (rc) {
+        delete P;
+        return rc;
     }
-    P->R = row;
     if (active_dof_mask) {
         P->mask.assign(active_dof_mask, active_dof_mask + D);
         for (float m : P->mask)
             if (m != 1.f) P->mask_any = 1;
     }
-    int rc = build_problem_blob(P);
+    rc = build_problem_blob(P);
     if (!rc) rc = upload_blob(P, nullptr);
     if (!rc) {
         const int rs = rec_stride(P->E);
@@ -807,7 +809,7 @@ int ik_solve_plain(IkProblem* P, int32_t batch, float* d_q, float* d_base, const
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid);
+        rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid, kBlockThreads);
         if (rc) return rc;
         for (int k = -1; k < prm.max_iter; ++k) {
             kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, P->d_rec, prm,
@@ -839,7 +841,7 @@ int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, 
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid);
+        rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, prm, P->d_queue, d_cost,
                                                       d_lambda, d_iters, d_status);
@@ -864,7 +866,7 @@ int ik_fk(IkRobot* R, int32_t batch, const float* d_q, const float* d_base, floa
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(R->d_blob[f], batch, d_q, d_base, d_T_joint, d_T_link,
                                                       d_S_world, d_spheres, d_link_bounds);
@@ -890,7 +892,7 @@ int ik_link_jacobian(IkRobot* R, int32_t batch, const float* d_q, const float* d
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(R->d_blob[f], batch, d_q, d_base, link, body_frame ? 1 : 0,
                                                       d_J);
@@ -914,7 +916,7 @@ int ik_residual_jacobian(IkProblem* P, int32_t batch, const float* d_q, const fl
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, d_r, d_J);
         rc = check_launch();
@@ -935,7 +937,7 @@ int ik_normal_equations(IkProblem* P, int32_t batch, const float* d_q, const flo
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, d_H, d_g, d_cost);
         rc = check_launch();
@@ -982,7 +984,7 @@ int ik_damped_solve(int32_t batch, int32_t dim, const float* d_H, const float* d
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(cache[dim], batch, d_H, d_g, d_lambda, d_delta, d_pred, d_spd);
         rc = check_launch();
@@ -1007,7 +1009,7 @@ int ik_step(IkProblem* P, int32_t batch, float* d_q, float* d_base, float* d_lam
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, d_lambda, prm, d_cost, d_delta,
                                                       d_pred, d_cost_new, d_accept);
@@ -1046,7 +1048,7 @@ int ik_metrics(IkRobot* R, int32_t batch, const float* d_q, const float* d_base,
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
         int grid = 0;
-        rc = grid_for(kfn, smem, batch, G, 0, grid);
+        rc = grid_for(kfn, smem, batch, G, 0, grid, kBlockThreads);
         if (rc) return rc;
         kfn<<<grid, kBlockThreads, smem, S(stream)>>>(R->d_blob[f], batch, d_q, d_base, num_targets, d_target_links,
                                                       d_targets, pos_threshold, rot_threshold, d_pos_err, d_rot_err,
