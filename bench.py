@@ -17,6 +17,7 @@ data path): each rank solves its own batch and rank 0 reports the aggregate.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -89,7 +90,9 @@ class Dist:
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class Clocks:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi samples (every 50 ms) kept for the wall-clock windows of the timed regions."""
+
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -97,6 +100,7 @@ class Clocks:
         self.idx = gpu_index
         self.proc = None
         self.path = None
+        self.windows = []
 
     def start(self):
         try:
@@ -104,35 +108,48 @@ class Clocks:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            t_end = time.time() + 5.0
+            while time.time() < t_end and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
+    def mark(self, t0: float, t1: float) -> None:
+        """Record one timed window [t0, t1] in host wall-clock seconds."""
+        self.windows.append((t0, t1))
+
     def stop(self) -> dict:
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        time.sleep(0.1)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(f[2]), float(f[3]), [n for n, v in zip(names, f[6:10])
+                                                              if v.lower() == "active"]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
         os.unlink(self.path)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(max(smax)) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if any(a - 0.06 <= r[0] <= b + 0.06 for a, b in self.windows)]
+        scope = "timed region"
+        if not inside:  # windows shorter than the sampling period: the whole loaded span
+            inside, scope = rows, "warm-up + timed region (timed windows shorter than the 50 ms sampling)"
+        sm = [r[1] for r in inside]
+        reasons = sorted({n for r in inside for n in r[3]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(r[2] for r in inside)) if inside else None,
+                "reasons": reasons, "samples": len(sm), "scope": scope}
 
 
 # ---------------------------------------------------------------------------
@@ -153,26 +170,58 @@ def converged_mask(N, cfg, q, base, pos=1e-3, rot=0.01):
     return ok.numpy().astype(bool), pe.numpy(), re.numpy()
 
 
-def time_solves(N, opt, vv, q_work, q0_dev, steps, warmup, flush):
-    """Device-resident timing: q reset on device, L2 flushed between steps, CUDA events around each solve."""
-    ev0, ev1 = N.Event(), N.Event()
+def _measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool (driver-written file), else the recipe's fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def _profiled_traffic(args, B):
+    """DRAM bytes per launch from the committed ncu summary, for the workload it was captured on."""
+    if args.config != "chain7c" or args.form != "persistent" or args.pair_mode != "all":
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "lm_persistent_kernel_chain7c.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    v = int(line.split(":")[1].split()[0])
+                    return v if B == 16384 else None
+    except OSError:
+        pass
+    return None
+
+
+def time_solves(N, opt, vv, q_work, q0_dev, steps, warmup, flush, clocks=None):
+    """Device-resident timing, L2 flushed between steps, CUDA events on the launching stream.
+
+    Returns (ms per step, ms per solve launch, library kernel launches in the timed region): a step is the
+    on-device reset of q to the start point plus one whole solve."""
+    ev0, ev1, ev2 = N.Event(), N.Event(), N.Event()
     for _ in range(warmup):
         q_work.assign(q0_dev)
         opt.solve(vv)
     N.synchronize()
     launches0 = N.launch_count()
-    total = 0.0
+    total = solve = 0.0
+    t0 = time.time()
     for _ in range(steps):
         flush.zero_()
         N.synchronize()
         ev0.record()
         q_work.assign(q0_dev)
-        opt.solve(vv)
         ev1.record()
+        opt.solve(vv)
+        ev2.record()
         N.synchronize()
-        total += ev0.elapsed_ms(ev1)
+        total += ev0.elapsed_ms(ev2)
+        solve += ev1.elapsed_ms(ev2)
+    if clocks is not None:
+        clocks.mark(t0, time.time())
     launches = N.launch_count() - launches0
-    return total / steps, launches
+    return total / steps, solve / steps, launches
 
 
 def run_b200(args, dist: Dist) -> dict:
@@ -206,8 +255,7 @@ def run_b200(args, dist: Dist) -> dict:
     clocks = Clocks(dist.local_rank % ndev)
     dist.barrier()
     clocks.start()
-    ms, launches = time_solves(N, opt, vv, state.q, q0_dev, args.steps, args.warmup, flush)
-    clk = clocks.stop()
+    ms, ms_kernel, launches = time_solves(N, opt, vv, state.q, q0_dev, args.steps, args.warmup, flush, clocks)
     ms_max = dist.reduce([ms], "max")[0]
 
     ok, pe, re = converged_mask(N, cfg, state.q, state.T_world_base if floating else None)
@@ -233,16 +281,25 @@ def run_b200(args, dist: Dist) -> dict:
         act_rows = float(np.mean(np.sum(r.numpy() > 0, axis=1)))
     wm = work_model(wl.spec, descs, floating, act_rows)
     f32, f64 = wm.solve_flops(iters, accepts)
-    t_s = ms * 1e-3
+    t_s = ms_kernel * 1e-3
     peak_eff = (f32 + f64) / (f32 / (p32.value * 1e12) + f64 / (p64.value * 1e12)) / 1e12
     achieved = (f32 + f64) / t_s / 1e12
+    # HBM side: bytes the solve must move (start point and targets in, solution and scalars out)
+    n_pose = sum(1 for t in cfg.terms if hasattr(t, "T_world_target"))
+    state_floats = wl.q0.shape[1] + (7 if floating else 0)
+    alg_bytes = B * (4 * 2 * state_floats + 4 * 7 * len(wl.target_links) * n_pose + 4 * 4)
+    hbm_peak = _measured_hbm_gbs()
     roofline = {
         "bound": "fp32",
         "achieved": round(achieved, 3),
         "peak": round(peak_eff, 3),
         "unit": "TFLOP/s",
         "frac": round(achieved / peak_eff, 4),
-        "traffic": None,
+        "traffic": _profiled_traffic(args, B),
+        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of this launch "
+                          "(profiles/lm_persistent_kernel_chain7c.md)",
+        "hbm": {"algorithmic_bytes": int(alg_bytes), "achieved_gbs": round(alg_bytes / t_s / 1e9, 2),
+                "peak_gbs": hbm_peak, "frac": round(alg_bytes / t_s / 1e9 / hbm_peak, 6) if hbm_peak else None},
         "peak_source": "measured FMA-chain FP32 %.1f / FP64 %.1f TFLOP/s (ik_measure_fma_peak), "
                        "weighted by this solve's FP32/FP64 work" % (p32.value, p64.value),
         "flops_fp32": f32,
@@ -262,6 +319,8 @@ def run_b200(args, dist: Dist) -> dict:
     bi = pin_q0.array.nbytes + len(pose_terms) * pin_t.array.nbytes
     bo = pin_q.array.nbytes + pin_c.array.nbytes
     for k in range(args.warmup + args.steps):
+        if k == args.warmup:
+            t_e2e = time.time()
         flush.zero_()
         N.synchronize()
         ev0.record()
@@ -275,6 +334,8 @@ def run_b200(args, dist: Dist) -> dict:
         N.synchronize()
         if k >= args.warmup:
             e2e_ms += ev0.elapsed_ms(ev1)
+    clocks.mark(t_e2e, time.time())
+    clk = clocks.stop()
     e2e_ms /= args.steps
     e2e_max = dist.reduce([e2e_ms], "max")[0]
     e2e = {"value": round(conv_total / (e2e_max * 1e-3), 1), "unit": UNIT, "h2d_bytes_per_step": int(bi),
@@ -287,7 +348,7 @@ def run_b200(args, dist: Dist) -> dict:
         opt_p = LMOptimizer(cfg.terms, lm_plain)
         st_p = cfg.robot.state(wl.q0, wl.base0)
         vvp = VarValues({VarKey.ROBOT: st_p})
-        ms_p, launches_p = time_solves(N, opt_p, vvp, st_p.q, q0_dev, max(3, args.steps // 2), 2, flush)
+        ms_p, _, launches_p = time_solves(N, opt_p, vvp, st_p.q, q0_dev, max(3, args.steps // 2), 3, flush)
         ms_p = dist.reduce([ms_p], "max")[0]
         okp, _, _ = converged_mask(N, cfg, st_p.q, st_p.T_world_base if floating else None)
         convp = dist.reduce([float(okp.sum())], "sum")[0]
@@ -324,7 +385,8 @@ def run_b200(args, dist: Dist) -> dict:
         "mean_iterations": round(float(iters.mean()), 2),
         "e2e": e2e,
         "roofline": roofline,
-        "gpu_launches": int(launches // args.steps),
+        "gpu_launches": int(launches),
+        "gpu_launches_per_step": int(launches // args.steps),
         "clocks": clk,
     }
     if plain is not None:
