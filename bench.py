@@ -47,6 +47,10 @@ def parse_args():
     p.add_argument("--form", choices=["persistent", "plain"], default="persistent")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
+    p.add_argument("--no-serve", action="store_true", help="skip the mixed-stream serving comparison")
+    p.add_argument("--serve-rate", type=float, default=100000.0, help="mixed stream arrival rate, problems/s")
+    p.add_argument("--serve-seconds", type=float, default=1.0, help="mixed stream duration")
+    p.add_argument("--serve-sweep", default="", help="comma-separated rates: print one serving line per rate")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU work of the baseline sample")
     return p.parse_args()
 
@@ -393,7 +397,32 @@ def run_b200(args, dist: Dist) -> dict:
         out["plain"] = plain
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(cfg, args.cpu_seconds, samples_only=False)
+    if dist.world == 1 and not args.no_serve:
+        out["serving"] = serve_compare(args.serve_rate, args.serve_seconds, args.seed)
     return out
+
+
+def serve_compare(rate: float, seconds: float, seed: int) -> dict:
+    """The mixed stream: four robots, log-uniform batch sizes in [1, 4096], Poisson arrivals of `rate`
+    problems/s, stop at 1e-4 m / 1e-3 rad or 100 iterations; served persistent form vs plain batches."""
+    from robokit_b200 import serve
+
+    types = serve.mixed_types(pool=4096, seed=seed)
+    srv = serve.make_server(types, slots=16384)
+    serve.run_served(srv, types, serve.make_stream(types, rate, 0.2, seed=seed + 1000))  # warm-up
+    reqs = serve.make_stream(types, rate, seconds, seed=seed)
+    served = serve.run_served(srv, types, reqs)
+    srv.close()
+    plain = serve.run_plain(types, reqs)
+    return {
+        "stream": f"4 robots (chain7, chain7c, humanoid, hand), Poisson {rate:.0f} problems/s for {seconds} s, "
+                  "batch log-uniform [1, 4096], stop 1e-4 m / 1e-3 rad, cap 100 iterations",
+        "rate": rate,
+        "served": served,
+        "plain": plain,
+        "converged_per_s_served_over_plain": round(served["converged_per_s"] / max(plain["converged_per_s"], 1e-9),
+                                                   3),
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -492,6 +521,16 @@ def main():
     args = parse_args()
     dist = Dist()
     try:
+        if args.serve_sweep and args.impl == "b200":
+            from robokit_b200 import _native as N
+
+            N.load_library()
+            N.check(N.lib().ik_set_device(dist.local_rank))
+            for rate in [float(x) for x in args.serve_sweep.split(",") if x]:
+                line = serve_compare(rate, args.serve_seconds, args.seed)
+                if dist.rank == 0:
+                    print(json.dumps({"serving_sweep": line}), flush=True)
+            return
         out = run_reference(args, dist) if args.impl == "reference" else run_b200(args, dist)
         if dist.rank == 0 and out:
             print(json.dumps(out), flush=True)

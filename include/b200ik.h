@@ -203,6 +203,48 @@ int ik_solve_persistent_noalloc(const IkRobotDesc* robot, int32_t floating_base,
 int ik_problem_set_schedule(IkProblem* problem, int32_t group_lanes, int32_t blocks_per_sm);
 int ik_problem_get_schedule(const IkProblem* problem, int32_t* group_lanes, int32_t* blocks_per_sm);
 
+/* ---- serving: continuous batching of requests ------------------------------
+ * The reference solves one batch per call (opt/optimizer.py:216-240); callers
+ * that receive IK requests over time (helpers/ik/ik.py:98-304 per request)
+ * wait for each batch.  A server keeps problem types resident and overlaps
+ * requests on the GPU: each type runs a persistent kernel whose lane groups
+ * take the next waiting problem as soon as theirs stops, so requests that
+ * arrive while others run are admitted as slots free up.  Inputs and results
+ * pass through mapped pinned host memory: submit, poll and fetch make no CUDA
+ * call except to relaunch a type's kernel after it exited idle.
+ * A server is used by one host thread. */
+typedef struct IkServer IkServer;
+/* budget_bytes bounds the memory of all types' slots (host-mapped inputs and
+ * outputs plus device tables); idle_us = how long a kernel with no work
+ * waits before it exits (0 = 200 us). */
+int ik_server_create(int64_t budget_bytes, int32_t idle_us, IkServer** out);
+/* Stops the kernels (after their running problems finish) and frees all. */
+int ik_server_destroy(IkServer* server);
+/* Register a problem type: robot + terms as for ik_problem_create, LM
+ * parameters, and `slots` = problems of this type that may be admitted at
+ * once.  The d_targets of pose terms are ignored: each request brings its
+ * own targets.  IK_E_OOM when the slots do not fit the budget. */
+int ik_server_add_type(IkServer* server, IkRobot* robot, int32_t floating_base, const IkTermDesc* terms,
+                       int32_t num_terms, const float* active_dof_mask, const IkLmParams* params, int32_t slots,
+                       int32_t* type_id);
+/* Submit `batch` problems of a type from host arrays (copied before return):
+ * h_q0 [batch, na], h_base0 [batch, 7] or NULL, h_targets = one array per
+ * pose term in term order, [batch, num_frames, 7].  A request that does not
+ * fit the free slots waits on the host and is admitted in arrival order as
+ * fetched requests release theirs.  IK_E_CAPACITY if batch > slots. */
+int ik_server_submit(IkServer* server, int32_t type, int32_t batch, const float* h_q0, const float* h_base0,
+                     const float* const* h_targets, int64_t* request_id);
+/* Report up to max_done newly finished requests (non-blocking). */
+int ik_server_poll(IkServer* server, int64_t* done_ids, int32_t max_done, int32_t* num_done);
+/* Copy a finished request's results (any pointer may be NULL) and release its
+ * slots: q [batch, na], base [batch, 7], cost, iterations, status as in
+ * ik_solve_persistent. */
+int ik_server_fetch(IkServer* server, int64_t request_id, float* h_q, float* h_base, float* h_cost,
+                    int32_t* h_iters, int32_t* h_status);
+/* Free slots, waiting and running requests, and kernel launches of a type. */
+int ik_server_info(IkServer* server, int32_t type, int32_t* free_slots, int32_t* pending, int32_t* inflight,
+                   int64_t* launches);
+
 /* ---- single-stage kernels (parity and the per-term reference API) ---------- */
 /* Forward kinematics, Robot.forward_kinematics (robo/robot.py:131) with the
  * motion subspace (robo/robot_kernels.py:651-664) and the collision spheres

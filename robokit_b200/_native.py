@@ -154,6 +154,20 @@ _SIGNATURES = {
         [ctypes.POINTER(IkRobotDesc), ctypes.c_int32, ctypes.POINTER(IkTermDesc), ctypes.c_int32, _vp,
          ctypes.c_int32, _vp, _vp, ctypes.POINTER(IkLmParams), _vp, _vp, _vp, _vp, _vp],
     ),
+    "ik_server_create": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "ik_server_destroy": (ctypes.c_int, [_vp]),
+    "ik_server_add_type": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int32, ctypes.POINTER(IkTermDesc), ctypes.c_int32, _vp, ctypes.POINTER(IkLmParams),
+         ctypes.c_int32, _i32p],
+    ),
+    "ik_server_submit": (
+        ctypes.c_int,
+        [_vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp, ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64)],
+    ),
+    "ik_server_poll": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32, _i32p]),
+    "ik_server_fetch": (ctypes.c_int, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    "ik_server_info": (ctypes.c_int, [_vp, ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.POINTER(ctypes.c_int64)]),
     "ik_fk": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ik_link_jacobian": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, ctypes.c_int32, ctypes.c_int32, _vp, _vp]),
     "ik_residual_jacobian": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]),

@@ -41,16 +41,29 @@ def needs_build() -> bool:
     return any(os.path.getmtime(s) > t for s in _sources())
 
 
+UNITS = ["ik_api.cu", "ik_noalloc.cu", "ik_server.cu"]
+
+
 def build_library(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit in parallel (nvcc -c), then link the shared library."""
     if not force and not needs_build():
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    units = [os.path.join(CSRC, "ik_api.cu"), os.path.join(CSRC, "ik_noalloc.cu")]
-    cmd = [nvcc, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", *units, "-o", OUT + ".tmp"]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    objs, procs = [], []
+    for u in UNITS:
+        obj = os.path.join(os.path.dirname(OUT), u.replace(".cu", ".o"))
+        cmd = [nvcc, *flags, f"-I{INCLUDE}", f"-I{CSRC}", "-c", os.path.join(CSRC, u), "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((u, subprocess.Popen(cmd)))
+        objs.append(obj)
+    failed = [u for u, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, f"nvcc {' '.join(failed)}")
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", OUT + ".tmp"],
+                   check=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -65,13 +65,6 @@ int fail(int code, const char* fmt, ...) {
 }  // namespace b200ik
 using host::fail;
 
-struct IkRobot {
-    RobotHost h;
-    char* d_blob[2] = {nullptr, nullptr};  // robot-only blobs: fixed base / floating base
-    int blob_bytes[2] = {0, 0};
-    int ws_bytes[2] = {0, 0};
-};
-
 struct IkProblem {
     IkRobot* robot = nullptr;
     int capacity = 0, floating = 0, D = 0, R = 0, E = 0;

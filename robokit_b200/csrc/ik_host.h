@@ -24,6 +24,21 @@ struct RobotHost {
     int fk_rounds = 0;
 };
 
+}  // namespace host
+}  // namespace b200ik
+
+// A robot registered with ik_robot_create: its host copy and the robot-only
+// table blobs (fixed base / floating base) used by the FK and Jacobian stages.
+struct IkRobot {
+    b200ik::host::RobotHost h;
+    char* d_blob[2] = {nullptr, nullptr};
+    int blob_bytes[2] = {0, 0};
+    int ws_bytes[2] = {0, 0};
+};
+
+namespace b200ik {
+namespace host {
+
 // One validated term descriptor with host copies of its arrays.
 struct TermHost {
     IkTermDesc d;

@@ -258,37 +258,51 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const c
     Ws w;
     const int gib = threadIdx.x / G;
     w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
-    // A warp claims one problem per group at once and its groups iterate in
-    // lockstep until all of them stop: groups that drift out of phase would
-    // make the warp issue each group's instruction stream separately.
-    constexpr int kGroupsPerWarp = 32 / G;
+    // Each group owns one problem at a time.  A group whose problem stops
+    // stores it and takes the next one from the queue at the top of the next
+    // round (the warp claims for all such groups with one atomic), so a warp
+    // never idles behind its slowest group while the queue still has work.
+    const unsigned full = 0xffffffffu;
     const int wg = (threadIdx.x & 31) / G;
+    int p = -1;
+    bool exhausted = false;
+    LmState st;
     while (true) {
-        int first = 0;
-        if ((threadIdx.x & 31) == 0) first = atomicAdd(queue, kGroupsPerWarp);
-        first = __shfl_sync(0xffffffffu, first, 0);
-        if (first >= batch) break;
-        const int p = first + wg;
-        const bool have = p < batch;
-        LmState st;
-        bool stop = true;
-        if (have) {
-            load_point<G>(g, t, w, p, q, base);
-            load_targets<G>(g, t, w, p, batch);
-            g.sync();
-            group_start<G>(g, t, w, st, P);
-            stop = (st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0;
+        const unsigned need = __ballot_sync(full, p < 0 && g.lane == 0);
+        if (need && !exhausted) {
+            int first = 0;
+            if ((threadIdx.x & 31) == 0) first = atomicAdd(queue, __popc(need));
+            first = __shfl_sync(full, first, 0);
+            if (first + __popc(need) >= batch) exhausted = true;
+            if (p < 0) {
+                const int np = first + __popc(need & ((1u << (wg * G)) - 1u));
+                if (np < batch) {
+                    p = np;
+                    load_point<G>(g, t, w, p, q, base);
+                    load_targets<G>(g, t, w, p, batch);
+                    g.sync();
+                    group_start<G>(g, t, w, st, P);
+                    if ((st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0) {
+                        if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
+                        store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
+                        g.sync();
+                        w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+                        p = -1;
+                    }
+                }
+            }
         }
-        while (__any_sync(0xffffffffu, !stop)) {
-            if (!stop) stop = group_iterate<G>(g, t, w, st, P);
+        if (!__any_sync(full, p >= 0)) {
+            if (exhausted) break;
+            continue;
         }
-        if (have) {
-            if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
+        if (p >= 0 && group_iterate<G>(g, t, w, st, P)) {
             store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
+            g.sync();
+            // restore the canonical buffer order (the accept path swaps q/qp and base/basep)
+            w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+            p = -1;
         }
-        __syncwarp();
-        // restore the canonical buffer order (the accept path swaps q/qp and base/basep)
-        w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
     }
 }
 }  // namespace b200ik

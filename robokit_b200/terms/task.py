@@ -112,6 +112,43 @@ def _destroy_problem(handle: int) -> None:
         pass
 
 
+def lower_terms(robot: Any, terms: List[ResidualTask], capacity: int, floating: bool,
+                keep: List[Any]) -> Any:
+    """IkTermDesc array for `terms`; the host arrays it points at are appended to `keep`."""
+
+    def arr(x: Any, dt: Any) -> Optional[int]:
+        if x is None:
+            return None
+        a = np.ascontiguousarray(x, dtype=dt)
+        if a.size == 0:
+            return None
+        keep.append(a)
+        return a.ctypes.data
+
+    descs = (N.IkTermDesc * max(1, len(terms)))()
+    var_stub = _VarStub(robot, capacity, floating)
+    for i, t in enumerate(terms):
+        d = t.native_desc(var_stub)
+        descs[i].kind = d["kind"]
+        descs[i].num_frames = d.get("num_frames", 0)
+        descs[i].frame_links = arr(d.get("frame_links"), np.int32)
+        descs[i].weights = arr(d.get("weights"), np.float32)
+        tg = d.get("targets")
+        if tg is not None:
+            keep.append(tg)
+            descs[i].d_targets = tg.ptr
+            descs[i].target_rows = tg.shape[0]
+        descs[i].margin = d.get("margin", 0.0)
+        descs[i].max_active_pairs = d.get("max_active_pairs", 0)
+        descs[i].pair_mode = d.get("pair_mode", 0)
+        descs[i].num_link_pairs = d.get("num_link_pairs", 0)
+        descs[i].link_pairs = arr(d.get("link_pairs"), np.int32)
+        descs[i].link_pair_offsets = arr(d.get("link_pair_offsets"), np.int32)
+        descs[i].num_sphere_pairs = d.get("num_sphere_pairs", 0)
+        descs[i].sphere_pairs = arr(d.get("sphere_pairs"), np.int32)
+    return descs
+
+
 class NativeProblem:
     """An IkProblem: robot + lowered term list, sized for `capacity` problems."""
 
@@ -120,27 +157,7 @@ class NativeProblem:
         import weakref
 
         self.keep: List[Any] = []
-        descs = (N.IkTermDesc * max(1, len(terms)))()
-        var_stub = _VarStub(robot, capacity, floating)
-        for i, t in enumerate(terms):
-            d = t.native_desc(var_stub)
-            descs[i].kind = d["kind"]
-            descs[i].num_frames = d.get("num_frames", 0)
-            descs[i].frame_links = self._arr(d.get("frame_links"), np.int32)
-            descs[i].weights = self._arr(d.get("weights"), np.float32)
-            tg = d.get("targets")
-            if tg is not None:
-                self.keep.append(tg)
-                descs[i].d_targets = tg.ptr
-                descs[i].target_rows = tg.shape[0]
-            descs[i].margin = d.get("margin", 0.0)
-            descs[i].max_active_pairs = d.get("max_active_pairs", 0)
-            descs[i].pair_mode = d.get("pair_mode", 0)
-            descs[i].num_link_pairs = d.get("num_link_pairs", 0)
-            descs[i].link_pairs = self._arr(d.get("link_pairs"), np.int32)
-            descs[i].link_pair_offsets = self._arr(d.get("link_pair_offsets"), np.int32)
-            descs[i].num_sphere_pairs = d.get("num_sphere_pairs", 0)
-            descs[i].sphere_pairs = self._arr(d.get("sphere_pairs"), np.int32)
+        descs = lower_terms(robot, terms, capacity, floating, self.keep)
         mask = None
         if active_dof_mask is not None:
             mask = np.ascontiguousarray(active_dof_mask, np.float32)
@@ -155,15 +172,6 @@ class NativeProblem:
         D, R, C = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         N.check(N.lib().ik_problem_info(self.handle, ctypes.byref(D), ctypes.byref(R), ctypes.byref(C)))
         self.tangent_dim, self.residual_dim = D.value, R.value
-
-    def _arr(self, x: Any, dt: Any) -> Optional[int]:
-        if x is None:
-            return None
-        a = np.ascontiguousarray(x, dtype=dt)
-        if a.size == 0:
-            return None
-        self.keep.append(a)
-        return a.ctypes.data
 
     def set_schedule(self, group_lanes: int = 0, blocks_per_sm: int = 0) -> None:
         N.check(N.lib().ik_problem_set_schedule(self.handle, int(group_lanes), int(blocks_per_sm)))

@@ -1,0 +1,108 @@
+"""The continuous-batching server (ik_server_*): results alone vs in the mix, admission, relaunch, errors."""
+
+import time
+
+import numpy as np
+import pytest
+
+from robokit_b200 import _native as N
+from robokit_b200 import serve
+from robokit_b200.opt import LMOptimizer, VarKey, VarValues
+
+pytestmark = pytest.mark.gpu
+
+
+def _pool_solution(st):
+    """Every problem of the type's pool solved in one persistent launch (problems are independent)."""
+    wl = st.cfg.workload
+    opt = LMOptimizer(st.cfg.terms, st.lm)
+    state = st.cfg.robot.state(wl.q0, wl.base0)
+    opt.solve(VarValues({VarKey.ROBOT: state}))
+    base = state.T_world_base.numpy() if state.has_floating_base else None
+    return {"q": state.q.numpy(), "base": base, "cost": opt.costs.numpy(), "iterations": opt.iterations.numpy()}
+
+
+def _submit(srv, types, r):
+    q0, base0, tg = serve._inputs(types[r.type_id], r)
+    return srv.submit(r.type_id, q0, tg, base0)
+
+
+def _close_to_pool(res, ref, r):
+    sl = slice(r.start, r.start + r.batch)
+    # the server kernel and the batch kernel are compiled separately; the
+    # tolerance covers a different FMA contraction choice, nothing else
+    np.testing.assert_allclose(res["q"], ref["q"][sl], rtol=0, atol=1e-4)
+    np.testing.assert_allclose(res["cost"], ref["cost"][sl], rtol=1e-4, atol=1e-9)
+    if ref["base"] is not None:
+        np.testing.assert_allclose(res["base"], ref["base"][sl], rtol=0, atol=1e-4)
+    assert np.mean(res["iterations"] == ref["iterations"][sl]) > 0.95
+
+
+def test_results_alone_equal_results_in_the_mix(gpu):
+    """Requests of four robots submitted back to back overlap on the GPU; each result equals the same
+    request served alone (bitwise) and the batch solve of the same problems (within tolerance)."""
+    types = serve.mixed_types(pool=512, seed=5)
+    refs = [_pool_solution(st) for st in types]
+    rng = np.random.default_rng(0)
+    reqs = []
+    for i in range(16):
+        k = i % 4
+        b = int(rng.integers(1, 160))
+        reqs.append(serve.RequestSpec(0.0, k, int(rng.integers(0, 512 - b)), b))
+    srv = serve.make_server(types)
+    ids = [_submit(srv, types, r) for r in reqs]
+    mixed = srv.wait(ids, timeout_s=120)
+    for r, i in zip(reqs, ids):
+        _close_to_pool(mixed[i], refs[r.type_id], r)
+    # the same requests one at a time through the same server
+    for r, i in list(zip(reqs, ids))[:6]:
+        j = _submit(srv, types, r)
+        alone = srv.wait([j], timeout_s=60)[j]
+        for key in ("q", "cost", "iterations", "status"):
+            np.testing.assert_array_equal(alone[key], mixed[i][key])
+    srv.close()
+
+
+def test_requests_wait_for_free_slots(gpu):
+    types = serve.mixed_types(pool=256, seed=9)[:2]
+    refs = [_pool_solution(st) for st in types]
+    srv = serve.make_server(types, slots=64)
+    reqs = [serve.RequestSpec(0.0, 1, 40 * i, 40) for i in range(5)] + [serve.RequestSpec(0.0, 0, 7, 64)]
+    ids = [_submit(srv, types, r) for r in reqs]
+    assert srv.info(1)["pending"] >= 3
+    out = srv.wait(ids, timeout_s=120)
+    for r, i in zip(reqs, ids):
+        _close_to_pool(out[i], refs[r.type_id], r)
+    info = srv.info(1)
+    assert info["free_slots"] == 64 and info["pending"] == 0 and info["inflight"] == 0
+    srv.close()
+
+
+def test_kernel_relaunches_after_idle_exit(gpu):
+    types = serve.mixed_types(pool=128, seed=3)[:1]
+    ref = _pool_solution(types[0])
+    srv = serve.make_server(types)
+    for start in (0, 50, 90):
+        r = serve.RequestSpec(0.0, 0, start, 30)
+        i = _submit(srv, types, r)
+        _close_to_pool(srv.wait([i], timeout_s=60)[i], ref, r)
+        time.sleep(0.05)  # far longer than the idle limit: the kernel exits
+    assert srv.info(0)["launches"] >= 2
+    srv.close()
+
+
+def test_server_errors(gpu):
+    types = serve.mixed_types(pool=64, seed=1)[:1]
+    srv = serve.make_server(types, slots=32)
+    q0, base0, tg = serve._inputs(types[0], serve.RequestSpec(0.0, 0, 0, 40))
+    with pytest.raises(N.NativeError, match="exceeds"):
+        srv.submit(0, q0, tg, base0)
+    with pytest.raises(ValueError, match="not registered"):
+        srv.submit(3, q0[:2], [t[:2] for t in tg], base0)
+    with pytest.raises(ValueError):
+        srv.submit(0, q0[:2], [t[:3] for t in tg], base0)
+    small = serve.IKServer(budget_bytes=1024)
+    with pytest.raises(N.NativeError, match="budget"):
+        small.add_type(types[0].cfg.robot, types[0].cfg.terms, types[0].lm, 4096)
+    small.close()
+    srv.close()
