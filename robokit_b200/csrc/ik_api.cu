@@ -127,18 +127,18 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_rlim = take(na * 4);
     h->w_Jc = take(kChunkRows * h->Dp * 4);
     h->w_rc = take(kChunkRows * 4);
-    h->w_rowmeta = take(kChunkRows * 4 * 4);
+    h->w_rowmeta = take(kChunkRows * 2 * 4);
     h->w_Hs = take(h->E * 4);
     h->w_Hc = take(h->E * 4);
-    h->w_L = take(h->T * 8);
-    h->w_tmp = take(D * 8);
-    h->w_y = take(D * 8);
+    h->w_L = take(D > kSmallD ? h->T * 8 : 0);  // small systems are factorised in registers
+    h->w_tmp = take(0);
+    h->w_y = take(0);
     h->w_q = take(na * 4);
     h->w_qp = take(na * 4);
     h->w_base = take(32);
     h->w_basep = take(32);
     h->w_d32 = take(D * 4);
-    h->w_misc = take(64 * 4);
+    h->w_misc = take((8 + h->ncoll) * 4);  // [8 + ci]: filled slots of collision term ci
     const int slots_off = take(ncoll_slots_bytes);
     h->ws_bytes = off;
     return slots_off;

@@ -267,7 +267,7 @@ struct Ws {
     IK_WS(float, rlim, w_rlim)        // limit residuals [na]
     IK_WS(float, Jc, w_Jc)            // Jacobian chunk [kChunkRows*Dp]
     IK_WS(float, rc, w_rc)            // chunk residuals [kChunkRows]
-    IK_WS(float, rowmeta, w_rowmeta)  // chunk row metadata [kChunkRows*4]: sphere i, sphere j, residual, spare
+    IK_WS(float, rowmeta, w_rowmeta)  // chunk row records [kChunkRows*2]: sphere pair i | j << 16, residual
     IK_WS(float, Hs, w_Hs)            // normal equations [E] (packed lower H, then g)
     IK_WS(float, Hc, w_Hc)            // compensation terms [E]
     IK_WS(double, L, w_L)             // Cholesky factor [T]
@@ -731,7 +731,14 @@ __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t
     g.sync();
 }
 
-// Build collision rows from rowmeta (i, j, residual) records into the chunk.
+// Chunk row record of a collision row: sphere pair (i | j << 16) and residual.
+__device__ __forceinline__ void rowmeta_put(Ws& w, int r, int si, int sj, float res) {
+    float* m = w.rowmeta() + 2 * r;
+    m[0] = __int_as_float(si | (sj << 16));
+    m[1] = res;
+}
+
+// Build collision rows from rowmeta (sphere pair, residual) records into the chunk.
 template <int G>
 __device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* S, const float* base,
                                      const CollEntry& ce, int nrows) {
@@ -739,8 +746,8 @@ __device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Ta
     const int items = nrows * D;
     for (int it = g.lane; it < items; it += G) {
         const int r = it / D, c = it - r * D;
-        const float* m = w.rowmeta() + 4 * r;
-        const int si = __float_as_int(m[0]), sj = __float_as_int(m[1]);
+        const int pk = __float_as_int(w.rowmeta()[2 * r]);
+        const int si = pk & 0xffff, sj = pk >> 16;
         const float4 a = *reinterpret_cast<const float4*>(w.sph() + 4 * si);
         const float4 b = *reinterpret_cast<const float4*>(w.sph() + 4 * sj);
         const V3 ci{a.x, a.y, a.z}, cj{b.x, b.y, b.z};
@@ -756,7 +763,7 @@ __device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Ta
         }
         w.Jc()[r * Dp + c] = val;
     }
-    for (int r = g.lane; r < nrows; r += G) w.rc()[r] = w.rowmeta()[4 * r + 2];
+    for (int r = g.lane; r < nrows; r += G) w.rc()[r] = w.rowmeta()[2 * r + 1];
     g.sync();
 }
 
@@ -798,10 +805,7 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
             for (int k0 = 0; k0 < nsl; k0 += kChunkRows) {
                 const int nr = min(kChunkRows, nsl - k0);
                 for (int r = g.lane; r < nr; r += G) {
-                    float* m = w.rowmeta() + 4 * r;
-                    m[0] = __int_as_float(slots[k0 + r].i);
-                    m[1] = __int_as_float(slots[k0 + r].j);
-                    m[2] = slots[k0 + r].r;
+                    rowmeta_put(w, r, slots[k0 + r].i, slots[k0 + r].j, slots[k0 + r].r);
                 }
                 g.sync();
                 group_collision_rows<G>(g, t, w, S, base, ce, nr);
@@ -830,10 +834,7 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
                     const int bit = __ffsll((long long)amask) - 1;
                     amask &= amask - 1ull;
                     const int pk = spk[bit * G + g.lane];
-                    float* m = w.rowmeta() + 4 * off++;
-                    m[0] = __int_as_float(pk & 0xffff);
-                    m[1] = __int_as_float(pk >> 16);
-                    m[2] = ce.weight * pair_penetration(w, pk, ce.margin);
+                    rowmeta_put(w, off++, pk & 0xffff, pk >> 16, ce.weight * pair_penetration(w, pk, ce.margin));
                 }
                 g.sync();
                 if (total > 0) {
@@ -854,10 +855,7 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
                     }
                     const unsigned bal = g.ballot(act);
                     if (act) {
-                        float* m = w.rowmeta() + 4 * (filled + __popc(bal & g.lt_mask()));
-                        m[0] = __int_as_float(pk & 0xffff);
-                        m[1] = __int_as_float(pk >> 16);
-                        m[2] = r;
+                        rowmeta_put(w, (filled + __popc(bal & g.lt_mask())), pk & 0xffff, pk >> 16, r);
                     }
                     filled += __popc(bal);
                     if (filled > kChunkRows - G) {
@@ -1007,11 +1005,22 @@ __device__ __forceinline__ bool group_small_solve(const Group<G>& g, const Tabs&
     return true;
 }
 
+// D > kSmallD: blocked right-looking factorisation in shared memory.  Per
+// block of kCholBlock columns every lane factorises the diagonal block
+// redundantly in registers, lanes solve the panel rows they own, then update
+// the trailing triangle element-parallel; two group syncs per block instead of
+// three per column.  The subtractions run in the same order as a column-by-
+// column right-looking factorisation.  The diagonal is stored as 1/L_kk.
+// Both triangular solves keep the right-hand side in registers of the lanes
+// that own its rows and broadcast each solved entry by shuffle (no syncs).
+constexpr int kCholBlock = 4;
+
 template <int G>
 __device__ __forceinline__ bool group_damped_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
                                    double& pred, double& dnorm) {
     const int D = t.h->D, T = t.h->T;
     if (D <= kSmallD) return group_small_solve<G>(g, t, w, Hp, lambda_f, pred, dnorm);
+    constexpr int B = kCholBlock;
     double* L = w.L();
     const double lam = (double)lambda_f;
     for (int e = g.lane; e < T; e += G) {
@@ -1020,69 +1029,133 @@ __device__ __forceinline__ bool group_damped_solve(const Group<G>& g, const Tabs
         if ((ab >> 8) == (ab & 0xff)) v += lam;
         L[e] = v;
     }
-    for (int i = g.lane; i < D; i += G) w.y()[i] = -(double)Hp[T + i];
     g.sync();
-    // Right-looking factorisation; the diagonal is stored as 1/L_kk so both
-    // triangular solves multiply instead of divide.
     bool ok = true;
-    for (int k = 0; k < D; ++k) {
-        const double akk = L[tri(k, k)];
-        if (!(akk > 0.0)) {
-            ok = false;
-            break;
+    for (int k0 = 0; k0 < D; k0 += B) {
+        const int bs = min(B, D - k0);
+        // diagonal block, identity-padded past D
+        double d[ctri(B, 0)];
+        sfor<B>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            sfor<i + 1>([&](auto J) {
+                constexpr int j = decltype(J)::value;
+                d[ctri(i, j)] = (i < bs) ? L[tri(k0 + i, k0 + j)] : ((i == j) ? 1.0 : 0.0);
+            });
+        });
+        sfor<B>([&](auto C) {
+            constexpr int c = decltype(C)::value;
+            double s = d[ctri(c, c)];
+            sfor<c>([&](auto M) { constexpr int m = decltype(M)::value; s -= d[ctri(c, m)] * d[ctri(c, m)]; });
+            ok = ok && (s > 0.0);
+            const double inv = rsqrt(s);
+            d[ctri(c, c)] = inv;
+            sfor<B - c - 1>([&](auto I0) {
+                constexpr int i = c + 1 + decltype(I0)::value;
+                double v = d[ctri(i, c)];
+                sfor<c>([&](auto M) { constexpr int m = decltype(M)::value; v -= d[ctri(i, m)] * d[ctri(c, m)]; });
+                d[ctri(i, c)] = v * inv;
+            });
+        });
+        if (!ok) break;  // every lane factorised the same block: a uniform decision
+        // panel rows below the block
+        for (int i = k0 + bs + g.lane; i < D; i += G) {
+            double* row = L + tri(i, k0);
+            double p[B];
+            sfor<B>([&](auto C) {
+                constexpr int c = decltype(C)::value;
+                if (c < bs) {
+                    double v = row[c];
+                    sfor<c>([&](auto M) { constexpr int m = decltype(M)::value; v -= p[m] * d[ctri(c, m)]; });
+                    p[c] = v * d[ctri(c, c)];
+                    row[c] = p[c];
+                }
+            });
         }
-        const double inv = rsqrt(akk);
-        g.sync();
-        for (int i = k + 1 + g.lane; i < D; i += G) {
-            const double l = L[tri(i, k)] * inv;
-            L[tri(i, k)] = l;
-            w.tmp()[i] = l;
+        if (g.lane == 0) {
+            sfor<B>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                sfor<i + 1>([&](auto J) {
+                    constexpr int j = decltype(J)::value;
+                    if (i < bs) L[tri(k0 + i, k0 + j)] = d[ctri(i, j)];
+                });
+            });
         }
-        if (g.lane == 0) L[tri(k, k)] = inv;
         g.sync();
-        // trailing update: each lane owns rows i = k+1+lane (mod G) and sweeps the
-        // contiguous packed row L[i][k+1..i] (independent updates, unrollable)
-        for (int i = k + 1 + g.lane; i < D; i += G) {
-            const double li = w.tmp()[i];
-            double* row = L + tri(i, 0);
-#pragma unroll 4
-            for (int j = k + 1; j <= i; ++j) row[j] -= li * w.tmp()[j];
+        // trailing triangle (i, j), k0+bs <= j <= i < D
+        const int base = k0 + bs, n = D - base;
+        const int nu = n * (n + 1) / 2;
+        for (int u = g.lane; u < nu; u += G) {
+            const unsigned ab = t.ab()[u];
+            const int i = base + (int)(ab >> 8), j = base + (int)(ab & 0xff);
+            const double* li = L + tri(i, k0);
+            const double* lj = L + tri(j, k0);
+            double v = L[tri(i, j)];
+            sfor<B>([&](auto C) {
+                constexpr int c = decltype(C)::value;
+                if (c < bs) v -= li[c] * lj[c];
+            });
+            L[tri(i, j)] = v;
         }
         g.sync();
     }
     if (!ok) {
-        g.sync();
-        for (int i = g.lane; i < D; i += G) {
-            w.y()[i] = 0.0;
-            w.d32()[i] = 0.f;
-        }
+        for (int i = g.lane; i < D; i += G) w.d32()[i] = 0.f;
         pred = 0.0;
         dnorm = 0.0;
         g.sync();
         return false;
     }
-    // forward substitution L z = -g (z into tmp; y[i] for i > k accumulates updates)
+    // right-hand side -g in the registers of the lanes owning its rows (i = lane + G r)
+    constexpr int R = (kMaxDim + G - 1) / G;
+    double yv[R];
+    sfor<R>([&](auto Rr) {
+        constexpr int r = decltype(Rr)::value;
+        const int i = g.lane + G * r;
+        yv[r] = (i < D) ? -(double)Hp[T + i] : 0.0;
+    });
+    // forward substitution L z = -g
     for (int k = 0; k < D; ++k) {
-        const double zk = w.y()[k] * L[tri(k, k)];
-        if (g.lane == 0) w.tmp()[k] = zk;
-        for (int i = k + 1 + g.lane; i < D; i += G) w.y()[i] -= L[tri(i, k)] * zk;
-        g.sync();
+        const int rk = k / G;
+        double yk = 0.0;
+        sfor<R>([&](auto Rr) {
+            constexpr int r = decltype(Rr)::value;
+            if (r == rk) yk = yv[r];
+        });
+        const double zk = __shfl_sync(g.mask, yk, k % G, G) * L[tri(k, k)];
+        sfor<R>([&](auto Rr) {
+            constexpr int r = decltype(Rr)::value;
+            const int i = g.lane + G * r;
+            if (i > k && i < D) yv[r] -= L[tri(i, k)] * zk;
+            else if (i == k) yv[r] = zk;
+        });
     }
-    // back substitution L^T x = z (x into y; tmp[i] for i < k accumulates updates)
+    // back substitution L^T x = z
     for (int k = D - 1; k >= 0; --k) {
-        const double xk = w.tmp()[k] * L[tri(k, k)];
-        if (g.lane == 0) w.y()[k] = xk;
-        for (int i = g.lane; i < k; i += G) w.tmp()[i] -= L[tri(k, i)] * xk;
-        g.sync();
+        const int rk = k / G;
+        double zk = 0.0;
+        sfor<R>([&](auto Rr) {
+            constexpr int r = decltype(Rr)::value;
+            if (r == rk) zk = yv[r];
+        });
+        const double xk = __shfl_sync(g.mask, zk, k % G, G) * L[tri(k, k)];
+        sfor<R>([&](auto Rr) {
+            constexpr int r = decltype(Rr)::value;
+            const int i = g.lane + G * r;
+            if (i < k) yv[r] -= L[tri(k, i)] * xk;
+            else if (i == k) yv[r] = xk;
+        });
     }
     double pp = 0.0, nn = 0.0;
-    for (int i = g.lane; i < D; i += G) {
-        const double x = w.y()[i];
-        const double gi = (double)Hp[T + i];
-        pp += x * (lam * x - gi);
-        nn += x * x;
-        w.d32()[i] = (float)x;
-    }
+    sfor<R>([&](auto Rr) {
+        constexpr int r = decltype(Rr)::value;
+        const int i = g.lane + G * r;
+        if (i < D) {
+            const double x = yv[r];
+            pp += x * (lam * x - (double)Hp[T + i]);
+            nn += x * x;
+            w.d32()[i] = (float)x;
+        }
+    });
     pred = 0.5 * g.sumd(pp);
     dnorm = sqrt(g.sumd(nn));
     g.sync();

@@ -232,11 +232,7 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 for (int k0 = 0; Jo && k0 < nsl; k0 += kChunkRows) {
                     const int nr = min(kChunkRows, nsl - k0);
                     for (int r = g.lane; r < nr; r += G) {
-                        float* m = w.rowmeta() + 4 * r;
-                        m[0] = __int_as_float(slots[k0 + r].i);
-                        m[1] = __int_as_float(slots[k0 + r].j);
-                        m[2] = slots[k0 + r].r;
-                        m[3] = __int_as_float(k0 + r);
+                        rowmeta_put(w, r, slots[k0 + r].i, slots[k0 + r].j, slots[k0 + r].r);
                     }
                     g.sync();
                     group_collision_rows<G>(g, t, w, S, b, ce, nr);
@@ -256,10 +252,7 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                         const float d = norm3(V3{a.x - bb.x, a.y - bb.y, a.z - bb.z});
                         const float pen = ce.margin - (d - a.w - bb.w);
                         const float res = ce.weight * fmaxf(0.f, pen);
-                        float* m = w.rowmeta() + 4 * r;
-                        m[0] = __int_as_float(pk & 0xffff);
-                        m[1] = __int_as_float(pk >> 16);
-                        m[2] = res;
+                        rowmeta_put(w, r, pk & 0xffff, pk >> 16, res);
                         if (ro) ro[ce.out_row + p0 + r] = res;
                     }
                     g.sync();
