@@ -126,7 +126,7 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_rpose = take(npose * 3 * 4);
     h->w_rlim = take(na * 4);
     h->w_Jc = take(kChunkRows * h->Dp * 4);
-    h->w_rc = take(kChunkRows * 4);
+    h->w_rc = take(0);
     h->w_rowmeta = take(kChunkRows * 2 * 4);
     h->w_Hs = take(h->E * 4);
     h->w_Hc = take(h->E * 4);
@@ -187,7 +187,7 @@ void build_robot_blob(const RobotHost& r, int floating, std::vector<char>& out, 
     h->base_off = floating ? 6 : 0;
     h->T = h->D * (h->D + 1) / 2;
     h->E = h->T + h->D;
-    h->Dp = h->D;
+    h->Dp = (h->D + 4) & ~3;  // chunk row: D Jacobian columns + the residual, 16-byte rows
     std::vector<float> mask(h->D, 1.f);
     int o = b.addv(mask);
     b.hdr()->o_mask = o;
@@ -451,7 +451,7 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     h->base_off = boff;
     h->T = h->D * (h->D + 1) / 2;
     h->E = h->T + h->D;
-    h->Dp = h->D;
+    h->Dp = (h->D + 4) & ~3;  // chunk row: D Jacobian columns + the residual, 16-byte rows
     int mask_any = 0;
     for (float m : mask_in)
         if (m != 1.f) mask_any = 1;

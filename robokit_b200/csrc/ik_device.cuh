@@ -265,8 +265,7 @@ struct Ws {
     IK_WS(float, tgt, w_tgt)          // pose targets [npose*8]
     IK_WS(float, rpose, w_rpose)      // pose residuals [npose*3]
     IK_WS(float, rlim, w_rlim)        // limit residuals [na]
-    IK_WS(float, Jc, w_Jc)            // Jacobian chunk [kChunkRows*Dp]
-    IK_WS(float, rc, w_rc)            // chunk residuals [kChunkRows]
+    IK_WS(float, Jc, w_Jc)            // chunk rows [kChunkRows*Dp]: D Jacobian columns, then the residual
     IK_WS(float, rowmeta, w_rowmeta)  // chunk row records [kChunkRows*2]: sphere pair i | j << 16, residual
     IK_WS(float, Hs, w_Hs)            // normal equations [E] (packed lower H, then g)
     IK_WS(float, Hc, w_Hc)            // compensation terms [E]
@@ -679,26 +678,66 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
 // self_collision_task.py:325-385).  Result: w.Hs()[0:T] packed lower J^T J,
 // w.Hs()[T:T+D] J^T r.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int tri(int i, int j) { return (i * (i + 1)) / 2 + j; }
+
+// compile-time loop: f(std::integral_constant<int, I>) for I = 0..N-1
+template <typename F, int... I>
+__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void sfor(F&& f) {
+    sfor_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// J^T J and J^T r of one chunk.  The residual is column D of the chunk, so the
+// lower triangle of [J r]^T [J r] holds both.  Each lane owns 4x4 tiles of that
+// (D+1)-square triangle and keeps them in registers over the chunk's rows (two
+// 16-byte loads per row and tile), then merges them into the compensated sums.
+// Every entry is summed over rows in ascending order, as a per-entry loop would.
+constexpr int kTile = 4;
+
 template <int G>
 __device__ __forceinline__ void group_accumulate_chunk(const Group<G>& g, const Tabs& t, Ws& w, int nrows) {
     const TabHeader* h = t.h;
-    const int Dp = h->Dp, T = h->T, E = h->E;
-    for (int e = g.lane; e < E; e += G) {
-        float s = 0.f;
-        if (e < T) {
-            const unsigned ab = t.ab()[e];
-            const int a = ab >> 8, b = ab & 0xff;
-            const float* ja = w.Jc() + a;
-            const float* jb = w.Jc() + b;
-            for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], jb[r * Dp], s);
-        } else {
-            const float* ja = w.Jc() + (e - T);
-            for (int r = 0; r < nrows; ++r) s = fmaf(ja[r * Dp], w.rc()[r], s);
+    const int D = h->D, Dp = h->Dp, T = h->T;
+    const int nb = (D + kTile) / kTile;  // tile rows of the (D+1)-square triangle
+    const int ntiles = nb * (nb + 1) / 2;
+    const float* Jc = w.Jc();
+    for (int tl = g.lane; tl < ntiles; tl += G) {
+        const unsigned ab = t.ab()[tl];
+        const int bi = (int)(ab >> 8), bj = (int)(ab & 0xff);
+        float acc[kTile][kTile];
+        sfor<kTile>([&](auto U) {
+            sfor<kTile>([&](auto V) { acc[decltype(U)::value][decltype(V)::value] = 0.f; });
+        });
+        for (int r = 0; r < nrows; ++r) {
+            const float4 x = *reinterpret_cast<const float4*>(Jc + r * Dp + kTile * bi);
+            const float4 y = *reinterpret_cast<const float4*>(Jc + r * Dp + kTile * bj);
+            const float xa[kTile] = {x.x, x.y, x.z, x.w};
+            const float ya[kTile] = {y.x, y.y, y.z, y.w};
+            sfor<kTile>([&](auto U) {
+                constexpr int u = decltype(U)::value;
+                sfor<kTile>([&](auto V) {
+                    constexpr int v = decltype(V)::value;
+                    acc[u][v] = fmaf(xa[u], ya[v], acc[u][v]);
+                });
+            });
         }
-        float hs = w.Hs()[e], hc = w.Hc()[e];
-        kadd(hs, hc, s);
-        w.Hs()[e] = hs;
-        w.Hc()[e] = hc;
+        sfor<kTile>([&](auto U) {
+            constexpr int u = decltype(U)::value;
+            sfor<kTile>([&](auto V) {
+                constexpr int v = decltype(V)::value;
+                const int ra = kTile * bi + u, cb = kTile * bj + v;
+                if (ra <= D && cb <= ra && cb < D) {
+                    const int e = (ra < D) ? tri(ra, cb) : T + cb;
+                    float hs = w.Hs()[e], hc = w.Hc()[e];
+                    kadd(hs, hc, acc[u][v]);
+                    w.Hs()[e] = hs;
+                    w.Hc()[e] = hc;
+                }
+            });
+        });
     }
     g.sync();
 }
@@ -727,7 +766,7 @@ __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t
             J[2 * Dp] = pe.w[2] * om.z;
         }
     }
-    for (int r = g.lane; r < 3 * ne; r += G) w.rc()[r] = w.rpose()[3 * e0 + r];
+    for (int r = g.lane; r < 3 * ne; r += G) w.Jc()[r * Dp + D] = w.rpose()[3 * e0 + r];
     g.sync();
 }
 
@@ -763,7 +802,7 @@ __device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Ta
         }
         w.Jc()[r * Dp + c] = val;
     }
-    for (int r = g.lane; r < nrows; r += G) w.rc()[r] = w.rowmeta()[2 * r + 1];
+    for (int r = g.lane; r < nrows; r += G) w.Jc()[r * Dp + D] = w.rowmeta()[2 * r + 1];
     g.sync();
 }
 
@@ -913,7 +952,6 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
 // H packed lower in `Hp` (fp32), g in Hp[T:].  Step in w.y() (fp64) and w.d32().
 // Returns false when a pivot is not positive (delta = 0, pred = 0).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int tri(int i, int j) { return (i * (i + 1)) / 2 + j; }
 
 constexpr int kSmallD = 8;  // systems up to this size are factorised in registers
 
@@ -923,16 +961,6 @@ __host__ __device__ constexpr int ctri(int i, int j) { return (i * (i + 1)) / 2 
 // registers — left-looking Cholesky, forward and back substitution fully
 // unrolled — so the solve needs no shared memory and no synchronisation; all
 // lanes hold the same step.
-// compile-time loop: f(std::integral_constant<int, I>) for I = 0..N-1
-template <typename F, int... I>
-__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, I...>) {
-    (f(std::integral_constant<int, I>{}), ...);
-}
-template <int N, typename F>
-__device__ __forceinline__ void sfor(F&& f) {
-    sfor_impl(f, std::make_integer_sequence<int, N>{});
-}
-
 template <int G>
 __device__ __forceinline__ bool group_small_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
                                   double& pred, double& dnorm) {
