@@ -691,7 +691,7 @@ __device__ __forceinline__ void sfor(F&& f) {
 }
 
 // J^T J and J^T r of one chunk.  The residual is column D of the chunk, so the
-// lower triangle of [J r]^T [J r] holds both.  Each lane owns 4x4 tiles of that
+// lower triangle of [J r]^T [J r] holds both.  For D >= 16 each lane owns 4x4 tiles of that
 // (D+1)-square triangle and keeps them in registers over the chunk's rows (two
 // 16-byte loads per row and tile), then merges them into the compensated sums.
 // Every entry is summed over rows in ascending order, as a per-entry loop would.
@@ -701,6 +701,30 @@ template <int G>
 __device__ __forceinline__ void group_accumulate_chunk(const Group<G>& g, const Tabs& t, Ws& w, int nrows) {
     const TabHeader* h = t.h;
     const int D = h->D, Dp = h->Dp, T = h->T;
+    if (D < 4 * kTile) {
+        // small systems: one entry per lane at a time keeps all G lanes busy
+        const int E = h->E;
+        const float* Jr = w.Jc();
+        for (int e = g.lane; e < E; e += G) {
+            int a, b;
+            if (e < T) {
+                const unsigned ab = t.ab()[e];
+                a = (int)(ab >> 8);
+                b = (int)(ab & 0xff);
+            } else {
+                a = e - T;
+                b = D;
+            }
+            float s = 0.f;
+            for (int r = 0; r < nrows; ++r) s = fmaf(Jr[r * Dp + a], Jr[r * Dp + b], s);
+            float hs = w.Hs()[e], hc = w.Hc()[e];
+            kadd(hs, hc, s);
+            w.Hs()[e] = hs;
+            w.Hc()[e] = hc;
+        }
+        g.sync();
+        return;
+    }
     const int nb = (D + kTile) / kTile;  // tile rows of the (D+1)-square triangle
     const int ntiles = nb * (nb + 1) / 2;
     const float* Jc = w.Jc();
