@@ -46,6 +46,7 @@ def parse_args():
     p.add_argument("--pair-mode", choices=["all", "slots"], default="all")
     p.add_argument("--form", choices=["persistent", "plain"], default="persistent")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--lanes", type=int, default=0, help="lanes per problem (0 = automatic, 1, 8, 16 or 32)")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
     p.add_argument("--no-serve", action="store_true", help="skip the mixed-stream serving comparison")
     p.add_argument("--serve-rate", type=float, default=100000.0, help="mixed stream arrival rate, problems/s")
@@ -254,6 +255,9 @@ def run_b200(args, dist: Dist) -> dict:
     q0_dev = state.q.clone()
     vv = VarValues({VarKey.ROBOT: state})
     opt = LMOptimizer(cfg.terms, cfg.lm)
+    if args.lanes:
+        opt.reset(vv)
+        opt.set_schedule(args.lanes)
     flush = N.DeviceArray.empty(256 * 1024 * 1024 // 4)  # 256 MiB > 126 MB L2
 
     clocks = Clocks(dist.local_rank % ndev)
@@ -352,6 +356,9 @@ def run_b200(args, dist: Dist) -> dict:
         opt_p = LMOptimizer(cfg.terms, lm_plain)
         st_p = cfg.robot.state(wl.q0, wl.base0)
         vvp = VarValues({VarKey.ROBOT: st_p})
+        if args.lanes:
+            opt_p.reset(vvp)
+            opt_p.set_schedule(args.lanes)
         ms_p, _, launches_p = time_solves(N, opt_p, vvp, st_p.q, q0_dev, max(3, args.steps // 2), 3, flush)
         ms_p = dist.reduce([ms_p], "max")[0]
         okp, _, _ = converged_mask(N, cfg, st_p.q, st_p.T_world_base if floating else None)

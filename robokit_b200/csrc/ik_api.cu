@@ -13,6 +13,7 @@
 #include "b200ik.h"
 #include "ik_host.h"
 #include "ik_kernels.cuh"
+#include "ik_thread.cuh"
 
 using namespace b200ik;
 using host::ProblemTables;
@@ -20,6 +21,9 @@ using host::RobotHost;
 using host::TermHost;
 
 namespace {
+
+// whether automatic schedules pick one lane per problem where it applies
+constexpr bool kThreadByDefault = false;
 
 thread_local std::string g_last_error;
 std::atomic<long long> g_launches{0};
@@ -169,6 +173,7 @@ void add_robot_tables(BlobBuilder& b, const RobotHost& r) {
     o = b.addv(r.colstart); b.hdr()->o_colstart = o;
     o = b.addv(r.coljoint); b.hdr()->o_coljoint = o;
     o = b.addv(r.colmul); b.hdr()->o_colmul = o;
+    o = b.addv(r.jorder); b.hdr()->o_jorder = o;
 }
 
 std::vector<uint16_t> ab_table(int D) {
@@ -365,6 +370,13 @@ int b200ik::host::fill_robot(const IkRobotDesc* d, RobotHost& r) {
     int rounds = 0;
     while ((1 << rounds) < maxd) ++rounds;
     r.fk_rounds = rounds;
+    // topological order: by depth, ties in index order
+    std::vector<int> depth(nj, 0);
+    for (int j = 0; j < nj; ++j)
+        for (int cur = r.jparent[j]; cur != -1; cur = r.jparent[cur]) ++depth[j];
+    r.jorder.resize(nj);
+    for (int j = 0; j < nj; ++j) r.jorder[j] = j;
+    std::stable_sort(r.jorder.begin(), r.jorder.end(), [&](int a, int b) { return depth[a] < depth[b]; });
     return IK_OK;
 }
 
@@ -538,6 +550,32 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0, h->ncoll > 0);
     CollEntry* ce = reinterpret_cast<CollEntry*>(b.buf.data() + o_coll);
     for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
+    // lane-per-problem layout: small systems with all-pairs collision terms only
+    {
+        int off = 0;
+        auto take = [&](int n) {
+            const int o2 = off;
+            off += n;
+            return o2;
+        };
+        h->t_Tj = take(7 * h->nj);
+        h->t_S = take(6 * h->nj);
+        h->t_sph = take(h->ncoll > 0 ? 3 * h->ns : 0);
+        h->t_tgt = take(7 * h->npose);
+        h->t_Hs = take(h->E);
+        h->t_Hc = take(h->E);
+        h->t_q = take(std::max(h->na, 1));
+        h->t_qp = take(std::max(h->na, 1));
+        h->t_base = take(h->base_off ? 7 : 0);
+        h->t_basep = take(h->base_off ? 7 : 0);
+        bool ok = h->D <= kSmallD;
+        for (size_t i = 0; i < coll.size(); ++i) {
+            if (ce[i].mode != IK_PAIRS_ALL) ok = false;
+            ce[i].t_mask = take((ce[i].nsp + 31) / 32);
+        }
+        h->t_floats = off;
+        h->thread_ok = ok ? 1 : 0;
+    }
     h->bytes = (int)b.buf.size();
     out.blob = b.buf;
     out.blob_bytes = h->bytes;
@@ -659,8 +697,25 @@ int upload_blob(IkProblem* P, void* stream) {
     return IK_OK;
 }
 
+// lane-group width of the stage kernels (the lane-per-problem schedule only exists for solves)
 int problem_group(const IkProblem* P) {
-    return choose_group(P->D, P->blob_bytes, P->ws_bytes, P->group);
+    return choose_group(P->D, P->blob_bytes, P->ws_bytes, P->group == 1 ? 0 : P->group);
+}
+
+int thread_smem(const IkProblem* P) {
+    const TabHeader* h = reinterpret_cast<const TabHeader*>(P->blob.data());
+    return P->blob_bytes + kThreadBlock * h->t_floats * (int)sizeof(float);
+}
+
+bool thread_ok(const IkProblem* P) {
+    const TabHeader* h = reinterpret_cast<const TabHeader*>(P->blob.data());
+    return h->thread_ok && thread_smem(P) <= max_smem_optin();
+}
+
+// schedule of the whole-solve kernels: 1 = one lane per problem, else the group width
+int solve_lanes(const IkProblem* P) {
+    if ((P->group == 1 || (P->group == 0 && kThreadByDefault)) && thread_ok(P)) return 1;
+    return problem_group(P);
 }
 
 int check_batch(const IkProblem* P, int batch) {
@@ -769,10 +824,13 @@ int ik_problem_set_targets(IkProblem* P, int32_t term_index, const float* d_targ
 
 int ik_problem_set_schedule(IkProblem* P, int32_t group_lanes, int32_t blocks_per_sm) {
     if (!P) return fail(IK_E_INVALID, "problem is NULL");
-    if (group_lanes != 0 && group_lanes != 8 && group_lanes != 16 && group_lanes != 32)
-        return fail(IK_E_INVALID, "group_lanes %d not in {0, 8, 16, 32}", group_lanes);
+    if (group_lanes != 0 && group_lanes != 1 && group_lanes != 8 && group_lanes != 16 && group_lanes != 32)
+        return fail(IK_E_INVALID, "group_lanes %d not in {0, 1, 8, 16, 32}", group_lanes);
     if (blocks_per_sm < 0) return fail(IK_E_INVALID, "blocks_per_sm < 0");
-    if (group_lanes && smem_bytes(P->blob_bytes, P->ws_bytes, group_lanes) > max_smem_optin())
+    if (group_lanes == 1 && !thread_ok(P))
+        return fail(IK_E_UNSUPPORTED, "one lane per problem needs D <= %d, all-pairs collision terms and %d B of "
+                    "shared memory", kSmallD, thread_smem(P));
+    if (group_lanes > 1 && smem_bytes(P->blob_bytes, P->ws_bytes, group_lanes) > max_smem_optin())
         return fail(IK_E_UNSUPPORTED, "group width %d needs too much shared memory", group_lanes);
     P->group = group_lanes;
     P->blocks_per_sm = blocks_per_sm;
@@ -781,7 +839,7 @@ int ik_problem_set_schedule(IkProblem* P, int32_t group_lanes, int32_t blocks_pe
 
 int ik_problem_get_schedule(const IkProblem* P, int32_t* group_lanes, int32_t* blocks_per_sm) {
     if (!P) return fail(IK_E_INVALID, "problem is NULL");
-    if (group_lanes) *group_lanes = problem_group(P);
+    if (group_lanes) *group_lanes = solve_lanes(P);
     if (blocks_per_sm) *blocks_per_sm = P->blocks_per_sm;
     return IK_OK;
 }
@@ -795,9 +853,25 @@ int ik_solve_plain(IkProblem* P, int32_t batch, float* d_q, float* d_base, const
     if (!d_q && P->robot->h.na > 0) return fail(IK_E_INVALID, "q is NULL");
     if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
     if (batch == 0) return IK_OK;
+    const IkLmParams prm = *params;
+    if (solve_lanes(P) == 1) {
+        const int smem = thread_smem(P);
+        rc = prepare_kernel(lm_thread_plain_kernel, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(lm_thread_plain_kernel, smem, batch, 1, P->blocks_per_sm, grid, kThreadBlock);
+        if (rc) return rc;
+        for (int k = -1; k < prm.max_iter; ++k) {
+            lm_thread_plain_kernel<<<grid, kThreadBlock, smem, S(stream)>>>(
+                P->d_blob, batch, d_q, d_base, P->d_rec, prm, k < 0 ? 0 : 1, k < 0 ? 0 : k, P->d_counters, d_cost,
+                d_lambda, d_iters, d_status);
+            rc = check_launch();
+            if (rc) return rc;
+        }
+        return IK_OK;
+    }
     const int G = problem_group(P);
     const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
-    const IkLmParams prm = *params;
     IK_DISPATCH(G, lm_plain_kernel, {
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;
@@ -826,10 +900,22 @@ int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, 
     if (!d_q && P->robot->h.na > 0) return fail(IK_E_INVALID, "q is NULL");
     if (P->floating && !d_base) return fail(IK_E_INVALID, "floating base problem needs a base array");
     if (batch == 0) return IK_OK;
-    const int G = problem_group(P);
-    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
     const IkLmParams prm = *params;
     CK(cudaMemsetAsync(P->d_queue, 0, sizeof(int), S(stream)));
+    if (solve_lanes(P) == 1) {
+        const int smem = thread_smem(P);
+        rc = prepare_kernel(lm_thread_persistent_kernel, smem);
+        if (rc) return rc;
+        int grid = 0;
+        rc = grid_for(lm_thread_persistent_kernel, smem, batch, 1, P->blocks_per_sm, grid, kThreadBlock);
+        if (rc) return rc;
+        lm_thread_persistent_kernel<<<grid, kThreadBlock, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, prm,
+                                                                          P->d_queue, d_cost, d_lambda, d_iters,
+                                                                          d_status);
+        return check_launch();
+    }
+    const int G = problem_group(P);
+    const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
     IK_DISPATCH(G, lm_persistent_kernel, {
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;

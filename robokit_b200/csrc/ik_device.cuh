@@ -228,6 +228,7 @@ struct Tabs {
     IK_TAB(int, colstart, o_colstart)
     IK_TAB(int, coljoint, o_coljoint)
     IK_TAB(float, colmul, o_colmul)
+    IK_TAB(int, jorder, o_jorder)
     IK_TAB(PoseEntry, pose, o_pose)
     IK_TAB(CollEntry, coll, o_coll)
     IK_TAB(float, limw, o_limw)

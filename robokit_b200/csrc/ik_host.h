@@ -19,6 +19,7 @@ struct RobotHost {
     std::vector<int> jtype, jparent, jact, jmimic, lpj, sphlink;
     std::vector<float> jmul, joff, jaxis, jpt, lim, sph, lbound;
     std::vector<unsigned long long> lanc;  // per link: ancestor joints
+    std::vector<int> jorder;               // joints in topological order
     std::vector<int> colstart, coljoint;
     std::vector<float> colmul;
     int fk_rounds = 0;

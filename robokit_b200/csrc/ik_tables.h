@@ -50,7 +50,8 @@ struct CollEntry {
     int32_t rows;         // residual rows this term owns in the reference layout
     float margin;
     float weight;
-    int32_t pad[4];
+    int32_t t_mask;       // lane-per-problem workspace: first 32-bit activity word (all-pairs mode)
+    int32_t pad[3];
 };
 static_assert(sizeof(CollEntry) == 64, "CollEntry layout");
 
@@ -69,6 +70,7 @@ struct TabHeader {
     int32_t o_jtype, o_jparent, o_jact, o_jmimic, o_jmul, o_joff, o_jaxis, o_jpt;
     int32_t o_lpj, o_lanc, o_lbound, o_sph, o_sphlink, o_lim;
     int32_t o_colstart, o_coljoint, o_colmul;
+    int32_t o_jorder;     // joints in topological order (parents first)
     // problem tables
     int32_t o_pose, o_coll, o_limw, o_mask, o_ab;
     // per-group workspace layout (byte offsets inside one group's workspace)
@@ -78,7 +80,11 @@ struct TabHeader {
     int32_t w_q, w_qp, w_base, w_basep, w_d32, w_misc;
     int32_t Dp;           // padded row stride of the Jacobian chunk
     int32_t max_slots;    // sum of slot-mode K over collision terms
-    int32_t pad[4];
+    // lane-per-problem workspace (float offsets; float k of lane t at [k * blockDim + t])
+    int32_t thread_ok;    // 1 when the lane-per-problem kernels can run this problem
+    int32_t t_floats;
+    int32_t t_Tj, t_S, t_sph, t_tgt, t_Hs, t_Hc, t_q, t_qp, t_base, t_basep;
+    int32_t pad[2];
 };
 
 }  // namespace b200ik

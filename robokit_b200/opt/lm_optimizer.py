@@ -12,7 +12,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass, replace
-from typing import Any, Callable, List, Literal, Optional, Sequence, Tuple, Union
+from typing import Any, Callable, Dict, List, Literal, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -232,3 +232,53 @@ class LMOptimizer:
 
     def set_schedule(self, group_lanes: int = 0, blocks_per_sm: int = 0) -> None:
         self.problem.set_schedule(group_lanes, blocks_per_sm)
+
+    def autotune(self, var_values: VarValues, lanes: Sequence[int] = (1, 8, 16, 32),
+                 blocks_per_sm: Sequence[int] = (0,), repeats: int = 2) -> Dict[str, Any]:
+        """Time whole solves of `var_values` under each schedule that applies and keep the fastest.
+
+        A schedule is (lanes per problem, resident blocks per SM): one lane per
+        problem carries 32 problems per warp (small systems, throughput), wider
+        lane groups shorten each problem's iteration (latency).  The start point
+        is restored after every trial, so `var_values` is unchanged on return.
+        """
+        self.reset(var_values)
+        var = var_values.get(VarKey.ROBOT)
+        q0 = var.q.clone()
+        b0 = var.T_world_base.clone() if var.has_floating_base else None
+
+        def restore() -> None:
+            var.q.assign(q0)
+            if b0 is not None:
+                var.T_world_base.assign(b0)
+            var.invalidate()
+
+        ev0, ev1 = N.Event(), N.Event()
+        times: Dict[str, float] = {}
+        best, best_ms = None, float("inf")
+        for g in lanes:
+            for bps in blocks_per_sm:
+                try:
+                    self.set_schedule(g, bps)
+                except (N.NativeError, ValueError):
+                    continue
+                restore()
+                self.solve(var_values)  # warm-up: kernel attributes, caches
+                ms = 0.0
+                for _ in range(max(1, repeats)):
+                    restore()
+                    N.synchronize()
+                    ev0.record()
+                    self.solve(var_values)
+                    ev1.record()
+                    N.synchronize()
+                    ms += ev0.elapsed_ms(ev1)
+                ms /= max(1, repeats)
+                times[f"{g}x{bps}"] = round(ms, 4)
+                if ms < best_ms:
+                    best, best_ms = (g, bps), ms
+        if best is None:
+            raise RuntimeError("no schedule applies to this problem")
+        self.set_schedule(*best)
+        restore()
+        return {"lanes": best[0], "blocks_per_sm": best[1], "ms": round(best_ms, 4), "times_ms": times}
