@@ -129,18 +129,22 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_tgt = take(npose * 8 * 4);
     h->w_rpose = take(npose * 3 * 4);
     h->w_rlim = take(na * 4);
-    h->w_Jc = take(kChunkRows * h->Dp * 4);
+    // The Jacobian chunk and its row records live only inside a linearisation and
+    // the FP64 factor only inside a solve: they share one region.
+    const int chunk_bytes = al16(kChunkRows * h->Dp * 4) + al16(kChunkRows * 2 * 4);
+    const int factor_bytes = D > kSmallD ? h->T * 8 : 0;  // small systems are factorised in registers
+    h->w_Jc = take(std::max(chunk_bytes, factor_bytes));
+    h->w_rowmeta = h->w_Jc + al16(kChunkRows * h->Dp * 4);
+    h->w_L = h->w_Jc;
     h->w_rc = take(0);
-    h->w_rowmeta = take(kChunkRows * 2 * 4);
     h->w_Hs = take(h->E * 4);
     h->w_Hc = take(h->E * 4);
-    h->w_L = take(D > kSmallD ? h->T * 8 : 0);  // small systems are factorised in registers
     h->w_tmp = take(0);
     h->w_y = take(0);
     h->w_q = take(na * 4);
     h->w_qp = take(na * 4);
-    h->w_base = take(32);
-    h->w_basep = take(32);
+    h->w_base = take(h->base_off ? 32 : 0);
+    h->w_basep = take(h->base_off ? 32 : 0);
     h->w_d32 = take(D * 4);
     h->w_misc = take((8 + h->ncoll) * 4);  // [8 + ci]: filled slots of collision term ci
     const int slots_off = take(ncoll_slots_bytes);

@@ -320,6 +320,9 @@ def run_plain(types: Sequence[StreamType], reqs: Sequence[RequestSpec]) -> Dict[
 
 
 def _summary(types, reqs, results, lat, wall) -> Dict[str, Any]:
+    if not reqs:
+        return {"requests": 0, "problems": 0, "converged": 0, "wall_s": round(wall, 4), "solves_per_s": 0.0,
+                "converged_per_s": 0.0, "p50_ms": None, "p99_ms": None, "max_ms": None}
     problems = sum(r.batch for r in reqs)
     conv = sum(_converged(types, reqs[i], results[i]["q"], results[i]["base"]) for i in range(len(reqs)))
     return {

@@ -189,11 +189,18 @@ def test_oversized_group_is_refused(gpu):
     """A width whose workspaces do not fit one block's shared memory is an error, not a silent change."""
     from robokit_b200 import _native as N
 
-    cfg = configs.make("humanoid", 8)
-    opt = LMOptimizer(cfg.terms, cfg.lm)
-    opt.reset(VarValues({VarKey.ROBOT: cfg.robot.state(cfg.workload.q0, cfg.workload.base0)}))
+    from robokit_b200.robo.robot import Robot
+    from robokit_b200.robo.synthetic import serial_chain
+    from robokit_b200.terms.dense import PositionTask
+
+    spec = serial_chain(seed=1, dofs=60)  # 60x60 normal equations: one 8-lane workspace is ~35 KB
+    robot = Robot(spec)
+    targets = np.tile(np.array([0.1, 0.2, 0.3, 1, 0, 0, 0], np.float32), (4, 1, 1))
+    opt = LMOptimizer([PositionTask(robot, spec.num_links - 1, targets)], LMOptimizerConfig(max_iter=2))
+    opt.reset(VarValues({VarKey.ROBOT: robot.state(np.zeros((4, 60), np.float32))}))
     with pytest.raises(N.NativeError, match="shared memory"):
         opt.set_schedule(8)
+    opt.set_schedule(32)
 
 
 def test_nonfinite_start_is_reported(gpu):
