@@ -211,7 +211,7 @@ void build_robot_blob(const RobotHost& r, int floating, std::vector<char>& out, 
     out = b.buf;
 }
 
-int smem_bytes(int blob_bytes, int ws_bytes, int G) { return blob_bytes + (kBlockThreads / G) * ws_bytes; }
+int smem_bytes(int blob_bytes, int ws_bytes, int G) { return blob_bytes + (kBlockThreads / G) * ws_stride(ws_bytes, G); }
 
 int choose_group(int D, int blob_bytes, int ws_bytes, int requested) {
     if (requested) return requested;

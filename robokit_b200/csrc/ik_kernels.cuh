@@ -19,7 +19,7 @@ __global__ void __launch_bounds__(kBlockThreads) fk_kernel(const char* __restric
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int nj = h->nj, nl = h->nl, ns = h->ns;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kBlockThreads) link_jacobian_kernel(const char
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int D = h->D, boff = h->base_off;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int D = h->D, Dp = h->Dp, R = h->R_ref, boff = h->base_off;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kBlockThreads) normal_kernel(const char* __res
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int D = h->D, T = h->T;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kBlockThreads) damped_solve_kernel(const char*
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int D = h->D, T = h->T;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kBlockThreads) step_kernel(const char* __restr
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int D = h->D;
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kBlockThreads) step_kernel(const char* __restr
         }
         store_solution<G>(g, t, w, st, p, q, base, nullptr, nullptr, nullptr, nullptr);
         g.sync();
-        w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+        w.bind(group_ws<G>(wsbase, h, gib), h);
     }
 }
 
@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kBlockThreads) metrics_kernel(const char* __re
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
         load_point<G>(g, t, w, p, q, base);

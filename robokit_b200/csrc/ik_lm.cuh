@@ -71,68 +71,73 @@ __device__ __forceinline__ bool check_stop(LmState& st, const IkLmParams& P) {
     return stop;
 }
 
-// Start a solve at the loaded point: evaluate, linearise, set damping.
-template <int G>
-__device__ __forceinline__ void group_start(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P) {
-    const EvalOut ev = group_eval<G>(g, t, w, w.q, cur_base<G>(t, w));
-    st.cost = ev.cost;
-    st.pos_err = ev.max_pos;
-    st.rot_err = ev.max_rot;
-    st.lambda = P.lambda_init;
-    st.status = isfinite(ev.cost) ? IK_ST_RUNNING : IK_ST_NONFINITE;
-    st.iters = 0;
-    st.accepts = 0;
-    group_linearize<G>(g, t, w, ev, cur_base<G>(t, w));
-}
-
 struct StepTrace {  // optional per-step outputs (ik_step)
     float cost_before, cost_new, pred;
     int accepted;
 };
 
-// One LM iteration from the cached linearisation (LMOptimizer._step_body,
-// lm_optimizer.py:834-1005).  Returns true when the problem stops.
+// One step of a problem's LM loop with a single call site for each heavy
+// phase (kernels that run both the start and the iterations keep one copy of
+// the evaluation and linearisation code, which keeps them in the instruction
+// cache).
+//  fresh: start at the loaded point — evaluate, set the damping, linearise;
+//         returns false (the caller applies its start rules).
+//  else:  one LM iteration from the cached linearisation (LMOptimizer._step_body,
+//         lm_optimizer.py:834-1005); returns true when the problem stops.
 template <int G>
-__device__ __forceinline__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
-                              StepTrace* trace = nullptr) {
-    double pred = 0.0, dnorm = 0.0;
-    const bool ok = group_damped_solve<G>(g, t, w, w.Hs(), st.lambda, pred, dnorm);
-    if (!ok) st.status |= IK_ST_NOT_SPD;
-    if ((P.stop_rules & IK_STOP_STEP) && ok && dnorm < (double)P.step_tol && trace == nullptr) {
-        st.status |= IK_ST_CONVERGED;
-        return true;
-    }
+__device__ __forceinline__ bool group_step(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
+                                           bool fresh, StepTrace* trace = nullptr) {
     const bool floating = t.h->base_off != 0;
-    group_integrate<G>(g, t, w, w.q, w.base, w.qp, w.basep);
-    const EvalOut ev = group_eval<G>(g, t, w, w.qp, floating ? w.basep : nullptr);
-    // gain ratio in FP64 (lm_optimizer.py:319-329)
-    bool acc = pred > 0.0;
-    if (acc) {
-        const double rho = ((double)st.cost - (double)ev.cost) / (pred + (double)P.gain_ratio_epsilon);
-        acc = rho >= (double)P.rho_min;
+    double pred = 0.0, dnorm = 0.0;
+    if (!fresh) {
+        const bool ok = group_damped_solve<G>(g, t, w, w.Hs(), st.lambda, pred, dnorm);
+        if (!ok) st.status |= IK_ST_NOT_SPD;
+        if ((P.stop_rules & IK_STOP_STEP) && ok && dnorm < (double)P.step_tol && trace == nullptr) {
+            st.status |= IK_ST_CONVERGED;
+            return true;
+        }
+        group_integrate<G>(g, t, w, w.q, w.base, w.qp, w.basep);
     }
-    if (trace) {
-        trace->cost_before = st.cost;
-        trace->cost_new = ev.cost;
-        trace->pred = (float)pred;
-        trace->accepted = acc ? 1 : 0;
+    const EvalOut ev = group_eval<G>(g, t, w, fresh ? w.q : w.qp, floating ? (fresh ? w.base : w.basep) : nullptr);
+    bool acc = true;
+    if (!fresh) {
+        // gain ratio in FP64 (lm_optimizer.py:319-329)
+        acc = pred > 0.0;
+        if (acc) {
+            const double rho = ((double)st.cost - (double)ev.cost) / (pred + (double)P.gain_ratio_epsilon);
+            acc = rho >= (double)P.rho_min;
+        }
+        if (trace) {
+            trace->cost_before = st.cost;
+            trace->cost_new = ev.cost;
+            trace->pred = (float)pred;
+            trace->accepted = acc ? 1 : 0;
+        }
     }
     if (acc) {
-        float* tq = w.q;
-        w.q = w.qp;
-        w.qp = tq;
-        float* tb = w.base;
-        w.base = w.basep;
-        w.basep = tb;
+        if (fresh) {
+            st.lambda = P.lambda_init;
+            st.status = isfinite(ev.cost) ? IK_ST_RUNNING : IK_ST_NONFINITE;
+            st.iters = 0;
+            st.accepts = 0;
+        } else {
+            float* tq = w.q;
+            w.q = w.qp;
+            w.qp = tq;
+            float* tb = w.base;
+            w.base = w.basep;
+            w.basep = tb;
+            st.lambda = fmaxf(st.lambda / P.lambda_factor, P.lambda_min);
+            st.accepts += 1;
+        }
         st.cost = ev.cost;
         st.pos_err = ev.max_pos;
         st.rot_err = ev.max_rot;
-        st.lambda = fmaxf(st.lambda / P.lambda_factor, P.lambda_min);
-        st.accepts += 1;
         group_linearize<G>(g, t, w, ev, floating ? w.base : nullptr);
     } else {
         st.lambda = fminf(fmaxf(st.lambda * P.lambda_factor, P.lambda_min), P.lambda_max);
     }
+    if (fresh) return false;
     st.iters += 1;
     bool stop = check_stop<G>(st, P);
     if (!stop && st.iters >= P.max_iter) {
@@ -140,6 +145,33 @@ __device__ __forceinline__ bool group_iterate(const Group<G>& g, const Tabs& t, 
         stop = true;
     }
     return stop;
+}
+
+// Start a solve at the loaded point: evaluate, linearise, set damping.
+template <int G>
+__device__ __forceinline__ void group_start(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P) {
+    group_step<G>(g, t, w, st, P, true);
+}
+
+// One LM iteration from the cached linearisation.  Returns true when the problem stops.
+template <int G>
+__device__ __forceinline__ bool group_iterate(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
+                                              StepTrace* trace = nullptr) {
+    return group_step<G>(g, t, w, st, P, false, trace);
+}
+
+// A problem that stops at its start point: apply the start rules, returns true to stop.
+template <int G>
+__device__ __forceinline__ bool start_stops(LmState& st, const IkLmParams& P) {
+    const bool stop = (st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0;
+    if (stop && st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
+    return stop;
+}
+
+// Workspace of lane group `gib`: groups are staggered across shared-memory banks.
+template <int G>
+__device__ __forceinline__ char* group_ws(char* wsbase, const TabHeader* h, int gib) {
+    return wsbase + (size_t)gib * ws_stride(h->ws_bytes, G);
 }
 
 template <int G>
@@ -186,7 +218,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_plain_kernel(const char* 
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const int ngroups = gridDim.x * (kBlockThreads / G);
     const int rs = rec_stride(h->E);
     for (int p = blockIdx.x * (kBlockThreads / G) + gib; p < batch; p += ngroups) {
@@ -196,12 +228,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_plain_kernel(const char* 
         bool touched = true;
         load_point<G>(g, t, w, p, q, base);
         load_targets<G>(g, t, w, p, batch);
-        if (mode == 0) {
-            g.sync();
-            group_start<G>(g, t, w, st, P);
-            check_stop<G>(st, P);
-            if (P.max_iter <= 0) st.status |= IK_ST_MAX_ITER;
-        } else {
+        if (mode == 1) {
             const RecScalars s = *rsc;
             st.cost = s.cost;
             st.lambda = s.lambda;
@@ -212,12 +239,16 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_plain_kernel(const char* 
             st.accepts = s.pad0;
             const bool done = (st.status & (IK_ST_CONVERGED | IK_ST_MAX_ITER | IK_ST_NONFINITE)) != 0;
             touched = !done;
-            if (!done) {
+            if (!done)
                 for (int e = g.lane; e < h->E; e += G) w.Hs()[e] = r[e];
-                g.sync();
-                group_iterate<G>(g, t, w, st, P);
-                // the all-problems rule decides the iteration count; without it the cap is max_iter
-            }
+        }
+        if (touched) {
+            g.sync();
+            group_step<G>(g, t, w, st, P, mode == 0);
+        }
+        if (mode == 0) {
+            check_stop<G>(st, P);
+            if (P.max_iter <= 0) st.status |= IK_ST_MAX_ITER;
         }
         if (all_rule && g.lane == 0 && mode == 1 && !(st.cost <= P.cost_tol)) atomicAdd(&counters[k % 3], 1);
         g.sync();
@@ -257,7 +288,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const c
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     // Each group owns one problem at a time.  A group whose problem stops
     // stores it and takes the next one from the queue at the top of the next
     // round (the warp claims for all such groups with one atomic), so a warp
@@ -265,7 +296,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const c
     const unsigned full = 0xffffffffu;
     const int wg = (threadIdx.x & 31) / G;
     int p = -1;
-    bool exhausted = false;
+    bool exhausted = false, fresh = false;
     LmState st;
     while (true) {
         const unsigned need = __ballot_sync(full, p < 0 && g.lane == 0);
@@ -278,17 +309,10 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const c
                 const int np = first + __popc(need & ((1u << (wg * G)) - 1u));
                 if (np < batch) {
                     p = np;
+                    fresh = true;
                     load_point<G>(g, t, w, p, q, base);
                     load_targets<G>(g, t, w, p, batch);
                     g.sync();
-                    group_start<G>(g, t, w, st, P);
-                    if ((st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0) {
-                        if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED)) st.status |= IK_ST_MAX_ITER;
-                        store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
-                        g.sync();
-                        w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
-                        p = -1;
-                    }
                 }
             }
         }
@@ -296,12 +320,17 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const c
             if (exhausted) break;
             continue;
         }
-        if (p >= 0 && group_iterate<G>(g, t, w, st, P)) {
-            store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
-            g.sync();
-            // restore the canonical buffer order (the accept path swaps q/qp and base/basep)
-            w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
-            p = -1;
+        if (p >= 0) {
+            bool stop = group_step<G>(g, t, w, st, P, fresh);
+            if (fresh) stop = start_stops<G>(st, P);
+            fresh = false;
+            if (stop) {
+                store_solution<G>(g, t, w, st, p, q, base, out_cost, out_lambda, out_iters, out_status);
+                g.sync();
+                // restore the canonical buffer order (the accept path swaps q/qp and base/basep)
+                w.bind(group_ws<G>(wsbase, h, gib), h);
+                p = -1;
+            }
         }
     }
 }

@@ -137,11 +137,12 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
     Group<G> g;
     Ws w;
     const int gib = threadIdx.x / G;
-    w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
+    w.bind(group_ws<G>(wsbase, h, gib), h);
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int wg = lane / G;
     int slot = -1, req = -1;
+    bool fresh = false;
     LmState st;
     long long idle_since = __shfl_sync(full, global_ns(), 0);
     while (true) {
@@ -182,17 +183,9 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
                     if (slot < 0 && rank < k) {
                         slot = es;
                         req = er;
+                        fresh = true;
                         load_request_point<G>(g, t, w, slot, c);
                         g.sync();
-                        group_start<G>(g, t, w, st, P);
-                        if ((st.status & IK_ST_NONFINITE) != 0 || check_stop<G>(st, P) || P.max_iter <= 0) {
-                            if (st.iters >= P.max_iter && !(st.status & IK_ST_CONVERGED))
-                                st.status |= IK_ST_MAX_ITER;
-                            finish_request_problem<G>(g, t, w, st, slot, req, c);
-                            g.sync();
-                            w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
-                            slot = -1;
-                        }
                     }
                 }
             }
@@ -225,11 +218,16 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
             continue;
         }
         idle_since = __shfl_sync(full, global_ns(), 0);
-        if (slot >= 0 && group_iterate<G>(g, t, w, st, P)) {
-            finish_request_problem<G>(g, t, w, st, slot, req, c);
-            g.sync();
-            w.bind(wsbase + (size_t)gib * h->ws_bytes, h);
-            slot = -1;
+        if (slot >= 0) {
+            bool stop = group_step<G>(g, t, w, st, P, fresh);
+            if (fresh) stop = start_stops<G>(st, P);
+            fresh = false;
+            if (stop) {
+                finish_request_problem<G>(g, t, w, st, slot, req, c);
+                g.sync();
+                w.bind(group_ws<G>(wsbase, h, gib), h);
+                slot = -1;
+            }
         }
     }
 }

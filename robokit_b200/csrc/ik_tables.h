@@ -8,6 +8,12 @@
 #pragma once
 #include <stdint.h>
 
+#ifdef __CUDACC__
+#define IK_HD __host__ __device__
+#else
+#define IK_HD
+#endif
+
 namespace b200ik {
 
 constexpr int kMaxJoints = 64;     // joint bit masks are one uint64
@@ -15,6 +21,11 @@ constexpr int kMaxLinks = 128;
 constexpr int kMaxDim = 64;        // tangent dimension (6 base + actuated)
 constexpr int kMaxSpheres = 1024;
 constexpr int kChunkRows = 32;     // Jacobian rows staged per accumulation chunk
+
+// Stride between the workspaces of consecutive lane groups of G lanes: whole
+// 128-byte lines plus 4 G bytes, so the groups of one warp sit on different
+// shared-memory banks (G < 32).
+IK_HD inline constexpr int ws_stride(int ws_bytes, int G) { return ((ws_bytes + 127) & ~127) + (G < 32 ? 4 * G : 0); }
 
 // pose-entry kinds
 constexpr int kPosePosition = 0;

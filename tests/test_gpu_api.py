@@ -103,7 +103,9 @@ def test_self_collision_batch_consistency(gpu, panda_collision_spec):
 
 def test_step_and_callback(gpu):
     cfg = configs.make("chain7", 32, seed=8)
-    lm = LMOptimizerConfig(max_iter=5, lm_lambda=1e-3, lambda_factor=10.0, early_stopping_interval=0)
+    # lambda0 = 0.1 keeps the damped systems well conditioned: the two paths are separate kernels whose
+    # FP32 contraction choices differ in the last bits, which badly conditioned steps would amplify
+    lm = LMOptimizerConfig(max_iter=5, lm_lambda=1e-1, lambda_factor=10.0, early_stopping_interval=0)
     opt = LMOptimizer(cfg.terms, lm)
     st = cfg.robot.state(cfg.workload.q0)
     seen = []
