@@ -49,6 +49,7 @@ def parse_args():
     p.add_argument("--lanes", type=int, default=0, help="lanes per problem (0 = automatic, 1, 8, 16 or 32)")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
     p.add_argument("--no-serve", action="store_true", help="skip the mixed-stream serving comparison")
+    p.add_argument("--no-ik", action="store_true", help="skip the IKSolver preset benchmark")
     p.add_argument("--serve-rate", type=float, default=100000.0, help="mixed stream arrival rate, problems/s")
     p.add_argument("--serve-seconds", type=float, default=1.0, help="mixed stream duration")
     p.add_argument("--serve-sweep", default="", help="comma-separated rates: print one serving line per rate")
@@ -406,7 +407,69 @@ def run_b200(args, dist: Dist) -> dict:
         out["cpu_baseline"] = cpu_baseline(cfg, args.cpu_seconds, samples_only=False)
     if dist.world == 1 and not args.no_serve:
         out["serving"] = serve_compare(args.serve_rate, args.serve_seconds, args.seed)
+    if dist.world == 1 and not args.no_ik:
+        out["ik_solver"] = ik_solver_bench()
     return out
+
+
+# the reference's published IKSolver(presets.basic) times on an RTX 4090 (scripts/benchmark/ik/results.csv)
+REFERENCE_IK_MS = {1: 0.646, 10: 0.610, 100: 0.813, 1000: 3.410, 2000: 7.124}
+
+
+def _panda_arm():
+    """The 7-DoF Panda of the reference's IK benchmark (finger joints fixed), from the committed fixture."""
+    from robokit_b200.robo.robot_spec import JointRecord, RobotSpec
+
+    with open(os.path.join(ROOT, "tests", "golden", "panda_golden.json")) as f:
+        g = json.load(f)["robot"]
+    joints = [JointRecord(**({**j, "type": "fixed", "mimic_joint": None} if j["type"] == "prismatic" else j))
+              for j in g["joints"]]
+    return RobotSpec.from_records(g["name"], g["links"], joints)
+
+
+def ik_solver_bench(batches=(1, 10, 100, 1000, 2000), runs: int = 5) -> dict:
+    """IKSolver(presets.basic) on FK-sampled Panda targets, the protocol of scripts/benchmark/ik/helper.py:124-160:
+    fresh targets per run, wall time of one batched solve (synchronised), success at 5 mm / 0.05 rad, 98th
+    percentile errors of the successful instances."""
+    from robokit_b200 import _native as N
+    from robokit_b200.helpers.ik import IKSolver, presets
+    from robokit_b200.robo.robot import Robot
+
+    spec = _panda_arm()
+    robot = Robot(spec)
+    link = spec.link_names.index("panda_hand")
+    rows = []
+    for B in batches:
+        ik = IKSolver(presets.basic, robot, "panda_hand")
+        targets = []
+        for r in range(runs):
+            q = robot.sample_q(B, seed=42 + r)
+            st = robot.forward_kinematics(robot.state(q))
+            targets.append(np.ascontiguousarray(st.get_T_world_link(link).numpy().reshape(B, 1, 7)))
+        ik.solve(targets[0])
+        N.synchronize()
+        times, succ, pos, rot = [], [], [], []
+        for T in targets:
+            t0 = time.perf_counter()
+            sol = ik.solve(T)
+            N.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+            m = ik.compute_metrics(sol, T)
+            ok = m.success
+            succ.append(100.0 * ok.mean())
+            if ok.any():
+                pos.append(float(np.percentile(m.position_error_m[ok, 0], 98)) * 1e3)
+                rot.append(float(np.percentile(m.orientation_error_rad[ok, 0], 98)))
+        ms = float(np.mean(times))
+        rows.append({"batch": B, "time_ms": round(ms, 4), "time_ms_std": round(float(np.std(times)), 4),
+                     "solves_per_s": round(B / (ms * 1e-3), 1), "success_pct": round(float(np.mean(succ)), 3),
+                     "pos_err_mm_p98": round(float(np.mean(pos)), 6) if pos else None,
+                     "ori_err_rad_p98": round(float(np.mean(rot)), 7) if rot else None,
+                     "reference_rtx4090_time_ms": REFERENCE_IK_MS.get(B)})
+    return {"workload": "IKSolver(presets.basic: 64 -> 4 -> 1 candidates, 6 + 10 LM iterations) on the 7-DoF Panda, "
+                        "one FK-sampled pose target per instance (target link panda_hand; the reference's benchmark "
+                        "uses panda_hand_tcp, 0.1034 m further along the hand axis), 5 runs per batch",
+            "rows": rows}
 
 
 def serve_compare(rate: float, seconds: float, seed: int) -> dict:

@@ -309,6 +309,16 @@ int ik_copy_rows(int32_t rows, int32_t width, const float* d_src, int64_t src_st
 int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, const float* d_src, float* d_dst,
                         void* stream);
 
+/* Keep the best `keep` of every instance's `num_candidates` candidates by cost
+ * (ascending, equal costs in candidate order, NaN last), the select of
+ * PopulationSolver (opt/population_solver.py:490-528).  Inputs are
+ * instance-major [batch*num_candidates]; outputs [batch*keep] gather q
+ * (num_actuated per row), base (7 per row; d_base may be NULL), cost and the
+ * picked candidate index (any output but q may be NULL). */
+int ik_select_best(int32_t batch, int32_t num_candidates, int32_t keep, const float* d_cost, const float* d_q,
+                   const float* d_base, int32_t num_actuated, float* d_q_out, float* d_base_out, float* d_cost_out,
+                   int32_t* d_index_out, void* stream);
+
 /* Clamp joints to [lo, hi], RobotState.clamp_q (robo/robot_state.py:314-333,
  * robot_kernels.py:593-609); entries whose d_mask is 0 are left (mask may be NULL). */
 int ik_clamp_q(int32_t batch, int32_t num_actuated, float* d_q, const float* d_limits, const float* d_mask,

@@ -188,6 +188,10 @@ _SIGNATURES = {
     ),
     "ik_copy_rows": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp]),
     "ik_masked_copy_rows": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp]),
+    "ik_select_best": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp],
+    ),
     "ik_clamp_q": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp]),
     "ik_malloc": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_size_t]),
     "ik_free": (ctypes.c_int, [_vp]),

@@ -1210,6 +1210,23 @@ int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, cons
     return check_launch();
 }
 
+int ik_select_best(int32_t batch, int32_t num_candidates, int32_t keep, const float* d_cost, const float* d_q,
+                   const float* d_base, int32_t num_actuated, float* d_q_out, float* d_base_out, float* d_cost_out,
+                   int32_t* d_index_out, void* stream) {
+    if (batch < 0) return fail(IK_E_INVALID, "batch < 0");
+    if (num_candidates < 1 || keep < 1 || keep > num_candidates)
+        return fail(IK_E_INVALID, "keep %d of %d candidates", keep, num_candidates);
+    if (num_actuated < 0 || num_actuated > kMaxDim) return fail(IK_E_INVALID, "num_actuated %d", num_actuated);
+    if (!d_cost || (num_actuated > 0 && (!d_q || !d_q_out)) || (d_base && !d_base_out))
+        return fail(IK_E_INVALID, "NULL array");
+    if (batch == 0) return IK_OK;
+    const int threads = 128;
+    const int blocks = (int)(((size_t)batch * 32 + threads - 1) / threads);
+    select_best_kernel<<<blocks, threads, 0, S(stream)>>>(batch, num_candidates, keep, d_cost, d_q, d_base, num_actuated,
+                                                        d_q_out, d_base_out, d_cost_out, d_index_out);
+    return check_launch();
+}
+
 int ik_clamp_q(int32_t batch, int32_t num_actuated, float* d_q, const float* d_limits, const float* d_mask,
                void* stream) {
     if (batch < 0 || num_actuated < 0) return fail(IK_E_INVALID, "negative size");

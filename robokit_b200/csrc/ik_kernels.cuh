@@ -529,3 +529,55 @@ __global__ void accept_kernel(int batch, float* cost, const float* cost_new, con
 }
 
 }  // namespace b200ik
+
+namespace b200ik {
+
+// Best `keep` of the `nc` candidates of every instance by cost, ascending,
+// equal costs in candidate order and NaN costs last (the select of
+// opt/population_solver.py:490-528).  One warp per instance: `keep` passes of
+// a warp arg-min over the candidates that come after the last pick in
+// (cost, index) order; the picks' points are gathered instance-major.
+__global__ void select_best_kernel(int batch, int nc, int keep, const float* __restrict__ cost,
+                                   const float* __restrict__ q, const float* __restrict__ base, int na,
+                                   float* __restrict__ q_out, float* __restrict__ base_out, float* __restrict__ cost_out,
+                                   int* __restrict__ idx_out) {
+    const int inst = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (inst >= batch) return;  // uniform per warp
+    const float* c = cost + (size_t)inst * nc;
+    float last_c = -INFINITY;
+    int last_i = -1;
+    for (int j = 0; j < keep; ++j) {
+        float bc = INFINITY;
+        int bi = 0x7fffffff;
+        for (int k = lane; k < nc; k += 32) {
+            float v = c[k];
+            if (!(v == v)) v = INFINITY;
+            const bool after = v > last_c || (v == last_c && k > last_i);
+            if (after && (v < bc || (v == bc && k < bi))) {
+                bc = v;
+                bi = k;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (oc < bc || (oc == bc && oi < bi)) {
+                bc = oc;
+                bi = oi;
+            }
+        }
+        last_c = bc;
+        last_i = bi;
+        const size_t src = (size_t)inst * nc + bi, dst = (size_t)inst * keep + j;
+        for (int a = lane; a < na; a += 32) q_out[dst * na + a] = q[src * na + a];
+        if (base && base_out && lane < 7) base_out[dst * 7 + lane] = base[src * 7 + lane];
+        if (lane == 0) {
+            if (cost_out) cost_out[dst] = c[bi];
+            if (idx_out) idx_out[dst] = bi;
+        }
+    }
+}
+
+}  // namespace b200ik

@@ -1,0 +1,7 @@
+"""Batched IK with a candidate population (robokit helpers/ik/)."""
+
+from . import presets
+from .config import IKContext, IKSolverConfig
+from .ik import IKMetrics, IKSolver
+
+__all__ = ["IKContext", "IKMetrics", "IKSolver", "IKSolverConfig", "presets"]

@@ -1,0 +1,60 @@
+"""Robot-free IK configuration (helpers/ik/config.py:12-80): term templates, candidate schedule, sampler."""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+from ...opt.lm_optimizer import LMOptimizerConfig
+from ...opt.population_solver import PopulationSolverConfig, Stage
+from ...opt.sampler import RobertsSamplerConfig
+from ...terms.task import Context, ResidualTask
+
+
+class IKContext(Context):
+    """Values an IKSolver gives its term templates (helpers/ik/config.py:12-32)."""
+
+    TARGET_LINKS = 0
+    TARGET_LINK = 1
+    TARGET = 2
+
+
+def _default_solver() -> PopulationSolverConfig:
+    """64 candidates for 6 iterations, the best 4 for 10 more, then the best one (helpers/ik/config.py:37-45)."""
+    return PopulationSolverConfig(
+        stages=[
+            Stage(6, 64, LMOptimizerConfig(lm_lambda=10.0)),
+            Stage(10, 4, LMOptimizerConfig(lm_lambda=1.0)),
+            Stage(0, 1),
+        ],
+        cuda_graph_mode="full",
+    )
+
+
+@dataclass
+class IKSolverConfig:
+    terms: List[ResidualTask] = field(default_factory=list)
+    score_terms: List[ResidualTask] = field(default_factory=list)
+    solver: PopulationSolverConfig = field(default_factory=_default_solver)
+    sampler: RobertsSamplerConfig = field(default_factory=lambda: RobertsSamplerConfig(keep_first=True))
+    base_init_sample_range: Tuple[float, float, float] = (0.1, 0.1, 0.0)
+    enable_T_world_base: bool = False
+    base_active_mask: Sequence[float] = (1.0, 1.0, 1.0, 1.0, 1.0, 1.0)
+
+    def __post_init__(self):
+        if len(self.base_active_mask) != 6:
+            raise ValueError(f"base_active_mask length {len(self.base_active_mask)} != 6")
+        if any(m != 1.0 for m in self.base_active_mask) and not self.enable_T_world_base:
+            raise ValueError("base_active_mask requires enable_T_world_base=True")
+
+    def add(self, term: ResidualTask, *, name: Optional[str] = None) -> "IKSolverConfig":
+        if name is not None:
+            term.name = name
+        self.terms.append(term)
+        return self
+
+    def add_score(self, term: ResidualTask, *, name: Optional[str] = None) -> "IKSolverConfig":
+        if name is not None:
+            term.name = name
+        self.score_terms.append(term)
+        return self

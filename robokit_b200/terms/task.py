@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import abc
 import ctypes
+from enum import Enum
 from typing import Any, Dict, List, Optional
 
 import numpy as np
@@ -19,8 +20,8 @@ from .. import _native as N
 from ..opt.var_values import VarKey, VarValues
 
 
-class Context:
-    """Placeholder values a helper fills in at build time (terms/task.py:41-63)."""
+class Context(Enum):
+    """Base of the placeholder keys a helper fills in at build time (terms/task.py:13-14)."""
 
 
 class Task(abc.ABC):

@@ -64,3 +64,18 @@ def gpu():
     n = N.device_count()
     assert n > 0, "GPU test selected but no CUDA device is visible"
     return N
+
+
+@pytest.fixture(scope="session")
+def panda_arm_spec(golden):
+    """The 7-DoF Panda of the reference's IK benchmark: finger joints fixed (scripts/benchmark/ik/helper.py:44-57)."""
+    from robokit_b200.robo.robot_spec import JointRecord, RobotSpec
+
+    g = golden["robot"]
+    joints = []
+    for j in g["joints"]:
+        rec = dict(j)
+        if rec["type"] == "prismatic":
+            rec.update(type="fixed", mimic_joint=None)
+        joints.append(JointRecord(**rec))
+    return RobotSpec.from_records(g["name"], g["links"], joints)

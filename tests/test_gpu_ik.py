@@ -1,0 +1,81 @@
+"""IKSolver over a candidate population: select kernel, presets on the Panda, stage plumbing, metrics."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from robokit_b200 import _native as N
+from robokit_b200.helpers.ik import IKSolver, presets
+from robokit_b200.opt import LMOptimizer, LMOptimizerConfig, VarKey, VarValues
+
+pytestmark = pytest.mark.gpu
+
+
+def test_select_best_matches_a_stable_sort(gpu):
+    rng = np.random.default_rng(0)
+    B, C, K, na = 37, 70, 5, 3
+    cost = rng.integers(0, 20, size=(B, C)).astype(np.float32)  # many ties
+    cost[rng.random((B, C)) < 0.05] = np.nan
+    q = rng.normal(size=(B * C, na)).astype(np.float32)
+    dc, dq = N.DeviceArray.from_numpy(cost.reshape(-1)), N.DeviceArray.from_numpy(q)
+    qo, co, io = N.DeviceArray.empty((B * K, na)), N.DeviceArray.empty(B * K), N.DeviceArray.empty(B * K, np.int32)
+    N.check(N.lib().ik_select_best(B, C, K, dc.ptr, dq.ptr, None, na, qo.ptr, None, co.ptr, io.ptr, None))
+    key = np.where(np.isnan(cost), np.inf, cost)
+    want = np.argsort(key, axis=1, kind="stable")[:, :K]
+    np.testing.assert_array_equal(io.numpy().reshape(B, K), want)
+    rows = (np.arange(B)[:, None] * C + want).reshape(-1)
+    np.testing.assert_array_equal(qo.numpy(), q[rows])
+    with pytest.raises(ValueError):
+        N.check(N.lib().ik_select_best(B, C, C + 1, dc.ptr, dq.ptr, None, na, qo.ptr, None, None, None, None))
+
+
+def _targets(robot, B, seed, link):
+    q = robot.sample_q(B, seed=seed)
+    st = robot.forward_kinematics(robot.state(q))
+    return st.get_T_world_link(link).numpy().reshape(B, 1, 7)
+
+
+def test_basic_preset_solves_panda_targets(gpu, panda_arm_spec):
+    """presets.basic (64 -> 4 -> 1 candidates) on FK-sampled Panda targets, scored at 5 mm / 0.05 rad
+    like scripts/benchmark/ik/helper.py:63-64."""
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_arm_spec)
+    link = panda_arm_spec.link_names.index("panda_hand")
+    ik = IKSolver(presets.basic, robot, "panda_hand")
+    assert ik.num_solutions == 1
+    T = _targets(robot, 128, 42, link)
+    sol = ik.solve(T)
+    assert sol.q.shape == (128, 7)
+    m = ik.compute_metrics(sol, T)
+    assert m.success.mean() >= 0.95, m.success.mean()
+    # the metrics kernel against the FP64 oracle
+    rob = oracle.Robot.from_spec(panda_arm_spec)
+    pe, re, ok = oracle.metrics(rob, sol.q.numpy(), None, [link], T, 0.005, 0.05)
+    np.testing.assert_allclose(m.position_error_m, pe, atol=2e-5)
+    np.testing.assert_allclose(m.orientation_error_rad, re, atol=2e-4)
+    # a second solve on new targets reuses the buffers
+    T2 = _targets(robot, 128, 43, link)
+    assert ik.compute_metrics(ik.solve(T2), T2).success.mean() >= 0.95
+    with pytest.raises(ValueError, match="Batch size mismatch"):
+        ik.solve(T2[:64])
+
+
+def test_single_stage_equals_the_optimizer(gpu, panda_arm_spec):
+    """One candidate, one stage: the solve is an LMOptimizer solve from the joint midrange (bitwise)."""
+    from robokit_b200.robo.robot import Robot
+    from robokit_b200.terms.dense import PositionLimit, PositionTask, RotationTask
+
+    robot = Robot(panda_arm_spec)
+    link = panda_arm_spec.link_names.index("panda_hand")
+    T = _targets(robot, 64, 7, link)
+    sol = IKSolver(presets.single_candidate, robot, link).solve(T).q.numpy()
+    terms = [PositionTask(robot, [link], T, weight=20.0), RotationTask(robot, [link], T, weight=10.0),
+             PositionLimit(robot, weight=50.0)]
+    opt = LMOptimizer(terms, LMOptimizerConfig(max_iter=30, lm_lambda=1.0, early_stopping_interval=0,
+                                               form="persistent"))
+    st = robot.state(np.tile(panda_arm_spec.midrange_q, (64, 1)).astype(np.float32))
+    opt.solve(VarValues({VarKey.ROBOT: st}))
+    np.testing.assert_array_equal(sol, st.q.numpy())
