@@ -341,6 +341,16 @@ int ik_event_create(void** event);
 int ik_event_destroy(void* event);
 int ik_event_record(void* event, void* stream);
 int ik_event_elapsed_ms(void* start, void* stop, float* ms);
+/* CUDA graphs of library calls: every call made on `stream` between begin and
+ * end (by this host thread) is recorded instead of run; launch replays them.
+ * The whole-solve "full" graph of OptimizerConfig.cuda_graph_mode
+ * (opt/optimizer.py:160-174, opt/population_solver.py:84-85).  The stream must
+ * be one from ik_stream_create; nothing may synchronise inside the capture.
+ * Pointers and sizes are frozen into the graph: replay it on the same buffers. */
+int ik_graph_begin(void* stream);
+int ik_graph_end(void* stream, void** graph);
+int ik_graph_launch(void* graph, void* stream);
+int ik_graph_destroy(void* graph);
 /* Count of this library's kernel launches since load (for launch accounting). */
 int ik_launch_count(int64_t* out);
 /* Measured CUDA-core FMA throughput (fp64 = 0: FP32, 1: FP64) in TFLOP/s on

@@ -209,6 +209,10 @@ _SIGNATURES = {
     "ik_event_destroy": (ctypes.c_int, [_vp]),
     "ik_event_record": (ctypes.c_int, [_vp, _vp]),
     "ik_event_elapsed_ms": (ctypes.c_int, [_vp, _vp, _f32p]),
+    "ik_graph_begin": (ctypes.c_int, [_vp]),
+    "ik_graph_end": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "ik_graph_launch": (ctypes.c_int, [_vp, _vp]),
+    "ik_graph_destroy": (ctypes.c_int, [_vp]),
     "ik_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int64)]),
     "ik_measure_fma_peak": (ctypes.c_int, [ctypes.c_int32, _f32p]),
 }
@@ -448,6 +452,30 @@ class Event:
         v = ctypes.c_float(0.0)
         check(lib().ik_event_elapsed_ms(self.handle, end.handle, ctypes.byref(v)))
         return float(v.value)
+
+
+class Graph:
+    """Library calls recorded on a stream between capture() and end(), replayed by launch()."""
+
+    def __init__(self, stream: "Stream"):
+        self.stream = stream
+        self.handle: Optional[int] = None
+        self._fin = None
+
+    def capture(self, body) -> "Graph":
+        check(lib().ik_graph_begin(self.stream.handle))
+        try:
+            body()
+        finally:
+            g = ctypes.c_void_p(0)
+            rc = lib().ik_graph_end(self.stream.handle, ctypes.byref(g))
+        check(rc)
+        self.handle = g.value
+        self._fin = weakref.finalize(self, lambda h=self.handle: _lib and _lib.ik_graph_destroy(ctypes.c_void_p(h)))
+        return self
+
+    def launch(self) -> None:
+        check(lib().ik_graph_launch(self.handle, self.stream.handle))
 
 
 class PinnedBuffer:

@@ -26,6 +26,7 @@ namespace {
 constexpr bool kThreadByDefault = false;
 
 thread_local std::string g_last_error;
+thread_local int g_capture_kernels = -1;  // >= 0 while this thread captures a graph
 std::atomic<long long> g_launches{0};
 
 #define CK(call)                                                                           \
@@ -223,7 +224,11 @@ int choose_group(int D, int blob_bytes, int ws_bytes, int requested) {
 int check_launch() {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(IK_E_CUDA, "kernel launch: %s", cudaGetErrorString(e));
-    g_launches.fetch_add(1);
+    // launches recorded into a graph under capture count when the graph runs
+    if (g_capture_kernels >= 0)
+        ++g_capture_kernels;
+    else
+        g_launches.fetch_add(1);
     return IK_OK;
 }
 
@@ -403,6 +408,60 @@ int ik_device_count(int* out) {
 
 int ik_set_device(int device) {
     CK(cudaSetDevice(device));
+    return IK_OK;
+}
+
+// ---- CUDA graphs of library calls --------------------------------------------
+struct IkGraph {
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+};
+
+int ik_graph_begin(void* stream) {
+    if (!stream) return fail(IK_E_INVALID, "capture needs a created stream, not the legacy default stream");
+    if (g_capture_kernels >= 0) return fail(IK_E_INVALID, "a capture is already open on this thread");
+    CK(cudaStreamBeginCapture(S(stream), cudaStreamCaptureModeThreadLocal));
+    g_capture_kernels = 0;
+    return IK_OK;
+}
+
+int ik_graph_end(void* stream, void** graph) {
+    if (!stream || !graph) return fail(IK_E_INVALID, "stream or out is NULL");
+    *graph = nullptr;
+    const int kernels = g_capture_kernels;
+    g_capture_kernels = -1;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(S(stream), &g);
+    if (e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return fail(IK_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    }
+    IkGraph* G = new IkGraph();
+    e = cudaGraphInstantiate(&G->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        delete G;
+        return fail(IK_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    G->kernels = kernels < 0 ? 0 : kernels;
+    *graph = G;
+    return IK_OK;
+}
+
+int ik_graph_launch(void* graph, void* stream) {
+    if (!graph) return fail(IK_E_INVALID, "graph is NULL");
+    IkGraph* G = static_cast<IkGraph*>(graph);
+    CK(cudaGraphLaunch(G->exec, S(stream)));
+    g_launches.fetch_add(G->kernels);
+    return IK_OK;
+}
+
+int ik_graph_destroy(void* graph) {
+    if (!graph) return IK_OK;
+    IkGraph* G = static_cast<IkGraph*>(graph);
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    delete G;
     return IK_OK;
 }
 

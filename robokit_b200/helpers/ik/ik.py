@@ -98,6 +98,8 @@ class IKSolver:
         self._targets = N.DeviceArray.zeros((B, self.num_targets, 7))
         self._terms = self._concrete_terms(self._targets)
         self._pose_terms = [t for t in self._terms if isinstance(t, _PoseTask)]
+        for t in self._pose_terms:  # every stage's problem reads the one target buffer
+            t.bind_targets(self._targets)
         self._stages = []
         for k, (width, lm) in enumerate(zip(self.widths, self.lm_configs)):
             iters = self.config.solver.stages[k].iters
@@ -113,9 +115,14 @@ class IKSolver:
         self._range = (lim[:, 1] - lim[:, 0]).astype(np.float32)
         self._sampler = RobertsSampler(C0, na, self.config.sampler.seed, self.config.sampler.keep_first)
         self._mid = N.DeviceArray.from_numpy(np.tile(spec.midrange_q.astype(np.float32), (B * C0, 1)))
+        # spread around the midrange (fixed, read by the captured graph) and around an init_state
+        self._noise_mid = N.DeviceArray.from_numpy(self._sampler.tangent(B, self._range))
         self._noise_scale = None
         self._noise = None
         self._cost = [N.DeviceArray.zeros(B * w) for w in self.widths]
+        self._params = [None if opt is None else opt.config.native_params() for (_, _, _, opt) in self._stages]
+        self._stream = N.Stream()
+        self._graph: Optional[N.Graph] = None
         self._batch = B
 
     def warmup(self, batch_size: int) -> None:
@@ -125,35 +132,70 @@ class IKSolver:
         N.synchronize()
 
     # --- solve ---------------------------------------------------------------------------
-    def _seed(self, init_state: Optional[RobotState], q_range: Union[float, Sequence[float]]) -> None:
+    def _seed_around(self, init_state: RobotState, q_range: Union[float, Sequence[float]], stream: int) -> None:
+        """Candidates spread around init_state's joints (helpers/ik/ik.py:486-540)."""
         B, C0 = self._batch, self.widths[0]
         na = self.num_joints
         state = self._stages[0][2]
-        if init_state is not None:
-            if init_state.batch_size != B:
-                raise ValueError(f"init_state batch size {init_state.batch_size} != {B}")
-            rep = np.repeat(np.arange(B, dtype=np.int32), C0)
-            center = N.DeviceArray.from_numpy(init_state.q.numpy()[rep])
-            scale = np.asarray(q_range, np.float32) * self._range
+        if init_state.batch_size != B:
+            raise ValueError(f"init_state batch size {init_state.batch_size} != {B}")
+        rep = np.repeat(np.arange(B, dtype=np.int32), C0)
+        center = N.DeviceArray.from_numpy(init_state.q.numpy()[rep])
+        if C0 == 1:
+            N.check(N.lib().ik_memcpy_dtod(state.q.ptr, center.ptr, center.nbytes, stream))
         else:
-            center = self._mid
-            scale = self._range.copy()
-        if C0 == 1 and init_state is not None:
-            state.q.assign(center)
-            return
-        if self._noise_scale is None or not np.array_equal(scale, self._noise_scale):
-            self._noise = N.DeviceArray.from_numpy(self._sampler.tangent(B, scale))
-            self._noise_scale = scale
-        N.check(N.lib().ik_integrate(B * C0, na, 0, center.ptr, None, self._noise.ptr, None, state.q.ptr, None, None))
-        state.invalidate()
-        state.clamp_q()
+            scale = np.asarray(q_range, np.float32) * self._range
+            if self._noise_scale is None or not np.array_equal(scale, self._noise_scale):
+                self._noise = N.DeviceArray.from_numpy(self._sampler.tangent(B, scale))
+                self._noise_scale = scale
+            N.check(N.lib().ik_integrate(B * C0, na, 0, center.ptr, None, self._noise.ptr, None, state.q.ptr, None,
+                                         stream))
+        N.check(N.lib().ik_clamp_q(B * C0, na, state.q.ptr, self.robot.limits_device().ptr, None, stream))
+        N.check(N.lib().ik_stream_synchronize(stream))  # `center` is freed on return
+
+    def _device_body(self, stream: int) -> None:
+        """Seed from the midrange, run every stage, select between stages: device work only, on `stream`."""
+        B, C0, na = self._batch, self.widths[0], self.num_joints
+        q0 = self._stages[0][2]
+        N.check(N.lib().ik_integrate(B * C0, na, 0, self._mid.ptr, None, self._noise_mid.ptr, None, q0.q.ptr, None,
+                                     stream))
+        N.check(N.lib().ik_clamp_q(B * C0, na, q0.q.ptr, self.robot.limits_device().ptr, None, stream))
+        self._run_stages(stream)
+
+    def _run_stages(self, stream: int) -> None:
+        B, na = self._batch, self.num_joints
+        for k, (width, iters, state, opt) in enumerate(self._stages):
+            if opt is not None:
+                n = B * width
+                opt._slice(n)
+                N.check(N.lib().ik_solve_persistent(opt.problem.handle, n, state.q.ptr, None,
+                                                    ctypes.byref(self._params[k]), self._cost[k].ptr, opt.lm.ptr,
+                                                    opt.iterations.ptr, opt.status.ptr, stream))
+            elif k == 0:
+                raise NotImplementedError("a first stage without iterations needs a scoring pass")
+            if k + 1 < len(self._stages):
+                nxt_w, _, nxt_state, _ = self._stages[k + 1]
+                N.check(N.lib().ik_select_best(B, width, nxt_w, self._cost[k].ptr, state.q.ptr, None, na,
+                                               nxt_state.q.ptr, None, self._cost[k + 1].ptr, None, stream))
+        for _, _, state, _ in self._stages:
+            state.invalidate()
 
     def solve(self, T_world_target: Any, init_state: Optional[RobotState] = None,
               out_state: Optional[RobotState] = None, init_sample_range: Optional[float] = None) -> RobotState:
-        """Solutions for every target, instance-major: (batch * num_solutions, dofs) (helpers/ik/ik.py:223-304)."""
-        T = N.as_device(T_world_target, np.float32)
-        if T.ndim == 2:
-            T = T.reshape((T.shape[0], 1, 7))
+        """Solutions for every target, instance-major: (batch * num_solutions, dofs) (helpers/ik/ik.py:223-304).
+
+        Under cuda_graph_mode "full" the device work of a solve from the midrange seed is captured into one
+        CUDA graph at the first solve and replayed after it; the call returns once the solutions are ready."""
+        if isinstance(T_world_target, np.ndarray) or not hasattr(T_world_target, "ptr"):
+            T = np.ascontiguousarray(T_world_target, np.float32)
+            if T.ndim == 2:
+                T = T.reshape(T.shape[0], 1, 7)
+            host = True
+        else:
+            T = N.as_device(T_world_target, np.float32)
+            if T.ndim == 2:
+                T = T.reshape((T.shape[0], 1, 7))
+            host = False
         if T.ndim != 3 or T.shape[2] != 7 or T.shape[1] != self.num_targets:
             raise ValueError(f"Target count ({T.shape[1] if T.ndim == 3 else '?'}) must match IK target count "
                              f"({self.num_targets})")
@@ -162,22 +204,25 @@ class IKSolver:
             self._build(B)
         elif B != self._batch:
             raise ValueError(f"Batch size mismatch: expected {self._batch}, got {B}")
-        self._targets.assign(T)
-        for t in self._pose_terms:
-            t.set_target(self._targets)
-        self._seed(init_state, self.config.sampler.scale if init_sample_range is None else init_sample_range)
-        na = self.num_joints
-        for k, (width, iters, state, opt) in enumerate(self._stages):
-            if opt is not None:
-                opt.solve(VarValues({VarKey.ROBOT: state}))
-                self._cost[k].assign(opt.costs)
-            elif k == 0:
-                self._score(state, self._cost[k])
-            if k + 1 < len(self._stages):
-                nxt_w, _, nxt_state, _ = self._stages[k + 1]
-                N.check(N.lib().ik_select_best(B, width, nxt_w, self._cost[k].ptr, state.q.ptr, None, na,
-                                               nxt_state.q.ptr, None, self._cost[k + 1].ptr, None, None))
-                nxt_state.invalidate()
+        st = self._stream.handle
+        nbytes = self._targets.nbytes
+        if host:
+            N.check(N.lib().ik_memcpy_htod(self._targets.ptr, T.ctypes.data, nbytes, st))
+        else:
+            N.check(N.lib().ik_memcpy_dtod(self._targets.ptr, T.ptr, nbytes, st))
+        if init_state is not None:
+            self._seed_around(init_state, self.config.sampler.scale if init_sample_range is None else init_sample_range,
+                              st)
+            self._run_stages(st)
+        elif self.config.solver.cuda_graph_mode == "full":
+            if self._graph is None:
+                self._device_body(st)  # the first solve runs directly (kernel set-up happens here)
+                self._graph = N.Graph(self._stream).capture(lambda: self._device_body(st))
+            else:
+                self._graph.launch()
+        else:
+            self._device_body(st)
+        N.check(N.lib().ik_stream_synchronize(st))
         final = self._stages[-1][2]
         if out_state is not None:
             out_state.q.assign(final.q)
@@ -189,11 +234,6 @@ class IKSolver:
     def costs(self) -> N.DeviceArray:
         """Cost of each returned solution (the final stage's)."""
         return self._cost[-1]
-
-    def _score(self, state: RobotState, out: N.DeviceArray) -> None:
-        opt = LMOptimizer(self._terms, LMOptimizerConfig(max_iter=0, early_stopping_interval=0, form="persistent"))
-        opt.solve(VarValues({VarKey.ROBOT: state}))
-        out.assign(opt.costs)
 
     # --- metrics ---------------------------------------------------------------------------
     def compute_metrics(self, state: RobotState, T_world_target: Any, position_threshold: float = 0.005,

@@ -111,6 +111,14 @@ class _PoseTask(ResidualTask):
             else:
                 self._target_host = new_h
 
+    def bind_targets(self, targets: N.DeviceArray) -> None:
+        """Read the targets from `targets` [rows, num_frames, 7] in place from now on (no copy per update)."""
+        if targets.ndim != 3 or targets.shape[1:] != (self.num_frames, 7):
+            raise ValueError(f"targets of shape {targets.shape} are not [rows, {self.num_frames}, 7]")
+        self._target_dev = targets
+        self._target_host = None
+        self._touch()
+
     @property
     def residual_dim(self) -> int:
         return 3 * self.num_frames

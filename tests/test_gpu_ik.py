@@ -79,3 +79,42 @@ def test_single_stage_equals_the_optimizer(gpu, panda_arm_spec):
     st = robot.state(np.tile(panda_arm_spec.midrange_q, (64, 1)).astype(np.float32))
     opt.solve(VarValues({VarKey.ROBOT: st}))
     np.testing.assert_array_equal(sol, st.q.numpy())
+
+
+def test_graph_replay_equals_direct_launches(gpu, panda_arm_spec):
+    """cuda_graph_mode "full" (one captured graph per solve) gives the solutions of direct launches, bitwise."""
+    import copy
+
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_arm_spec)
+    link = panda_arm_spec.link_names.index("panda_hand")
+    direct_cfg = copy.deepcopy(presets.basic)
+    direct_cfg.solver.cuda_graph_mode = "none"
+    graph = IKSolver(presets.basic, robot, "panda_hand")
+    direct = IKSolver(direct_cfg, robot, "panda_hand")
+    for seed in (11, 12, 13):  # the first graph solve runs directly, the next two replay the graph
+        T = _targets(robot, 96, seed, link)
+        n0 = N.launch_count()
+        a = graph.solve(T).q.numpy()
+        n1 = N.launch_count()
+        b = direct.solve(T).q.numpy()
+        np.testing.assert_array_equal(a, b)
+        assert n1 > n0  # replayed kernels are counted
+    assert graph._graph is not None and direct._graph is None
+
+
+def test_init_state_seeds_around_a_previous_solution(gpu, panda_arm_spec):
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_arm_spec)
+    link = panda_arm_spec.link_names.index("panda_hand")
+    ik = IKSolver(presets.basic, robot, "panda_hand")
+    T = _targets(robot, 32, 21, link)
+    first = ik.solve(T)
+    prev = robot.state(first.q.numpy())
+    again = ik.solve(T, init_state=prev, init_sample_range=0.05)
+    m = ik.compute_metrics(again, T)
+    assert m.success.mean() >= 0.95
+    with pytest.raises(ValueError, match="init_state batch size"):
+        ik.solve(T, init_state=robot.state(first.q.numpy()[:8]))
