@@ -367,6 +367,17 @@ def run_b200(args, dist: Dist) -> dict:
         plain = {"value": round(convp / (ms_p * 1e-3), 1), "ms_per_step": round(ms_p, 4),
                  "launches_per_step": launches_p // max(3, args.steps // 2),
                  "speedup_persistent_over_plain": round(ms_p / ms_max, 3)}
+        # the same plain solve recorded once as a CUDA graph and replayed (cuda_graph_mode "full")
+        lm_pg = LMOptimizerConfig(**{**cfg.lm.__dict__, "form": "plain", "cuda_graph_mode": "full"})
+        opt_pg = LMOptimizer(cfg.terms, lm_pg)
+        st_pg = cfg.robot.state(wl.q0, wl.base0)
+        vvg = VarValues({VarKey.ROBOT: st_pg})
+        if args.lanes:
+            opt_pg.reset(vvg)
+            opt_pg.set_schedule(args.lanes)
+        ms_g, _, _ = time_solves(N, opt_pg, vvg, st_pg.q, q0_dev, max(3, args.steps // 2), 3, flush)
+        ms_g = dist.reduce([ms_g], "max")[0]
+        plain["graph_ms_per_step"] = round(ms_g, 4)
 
     g, bps = opt.problem.schedule()
     out = {

@@ -115,6 +115,9 @@ class LMOptimizer:
         self._iter = 0
         self.max_batch_size = 0
         self.batch_size = 0
+        self._stream: Optional[N.Stream] = None
+        self._graph: Optional[N.Graph] = None
+        self._graph_key: Optional[tuple] = None
 
     # -- lifecycle ---------------------------------------------------------------------
     def _mask_np(self, D: int) -> Optional[np.ndarray]:
@@ -134,6 +137,7 @@ class LMOptimizer:
         B, D = capacity or var_values.batch_size, var_values.tangent_dim
         mask = self._mask_np(D)
         self._problem = NativeProblem(var.robot, self.terms, B, var.has_floating_base, mask)
+        self._graph = None  # a recorded solve names the old problem's buffers
         self._floating = var.has_floating_base
         self._robot = var.robot
         self.total_tangent_dim = D
@@ -192,10 +196,27 @@ class LMOptimizer:
             return var_values, self.costs
         prm = cfg.native_params()
         fn = N.lib().ik_solve_persistent if cfg.form == "persistent" else N.lib().ik_solve_plain
-        N.check(
-            fn(self._problem.handle, B, var.q.ptr, var.T_world_base.ptr if var.has_floating_base else None,
-               ctypes.byref(prm), self.costs.ptr, self.lm.ptr, self.iterations.ptr, self.status.ptr, None)
-        )
+        base = var.T_world_base.ptr if var.has_floating_base else None
+
+        def launch(stream: Optional[int]) -> None:
+            N.check(fn(self._problem.handle, B, var.q.ptr, base, ctypes.byref(prm), self.costs.ptr, self.lm.ptr,
+                       self.iterations.ptr, self.status.ptr, stream))
+
+        if cfg.cuda_graph_mode == "none":
+            launch(None)
+        else:
+            # the whole solve (one launch per iteration in the plain form) recorded once per set of buffers and
+            # parameters, then replayed (opt/optimizer.py:160-174, cuda_graph_mode)
+            if self._stream is None:
+                self._stream = N.Stream()
+            key = (B, var.q.ptr, base, self._problem.handle, self.costs.ptr, self.lm.ptr, bytes(prm))
+            if self._graph is None or self._graph_key != key:
+                launch(self._stream.handle)
+                self._graph = N.Graph(self._stream).capture(lambda: launch(self._stream.handle))
+                self._graph_key = key
+            else:
+                self._graph.launch()
+            self._stream.synchronize()
         var.invalidate()
         return var_values, self.costs
 

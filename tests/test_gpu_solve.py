@@ -231,3 +231,25 @@ def test_pose_stop_rule(gpu):
     assert conv.mean() > 0.5
     assert np.all(ok[conv])
     assert np.all(iters[~conv] == 100)
+
+
+@pytest.mark.parametrize("form", ["plain", "persistent"])
+def test_graph_mode_equals_direct_launches(gpu, form):
+    """cuda_graph_mode "full": the solve is recorded once and replayed; results equal direct launches bitwise."""
+    cfg = configs.make("chain7c", 200, seed=6)
+    outs = []
+    for mode in ("none", "full"):
+        lm = LMOptimizerConfig(**{**cfg.lm.__dict__, "form": form, "cuda_graph_mode": mode})
+        opt = LMOptimizer(cfg.terms, lm)
+        st = cfg.robot.state(cfg.workload.q0)
+        res = []
+        for _ in range(2):  # the second "full" solve replays the recorded graph
+            st.q.copy_from_numpy(cfg.workload.q0)
+            opt.solve(VarValues({VarKey.ROBOT: st}))
+            res.append((st.q.numpy(), opt.costs.numpy(), opt.iterations.numpy()))
+        outs.append(res)
+        if mode == "full":
+            assert opt._graph is not None
+    for a, b in zip(outs[0], outs[1]):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
