@@ -768,27 +768,53 @@ __device__ __forceinline__ void group_accumulate_chunk(const Group<G>& g, const 
 }
 
 // Build the Jacobian of pose entries [e0, e0+ne) into the chunk (3 rows each).
+// A lane owns a tangent column and walks the entries: a column driven by one
+// joint (the usual case) loads that joint's twist once and only tests, per
+// entry, whether the joint is an ancestor of the entry's link.
 template <int G>
 __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* Tj, const float* S,
                                 const float* base, int e0, int ne) {
-    const int D = t.h->D, Dp = t.h->Dp;
-    const int items = ne * D;
-    for (int it = g.lane; it < items; it += G) {
-        const int el = it / D, c = it - el * D;
-        const PoseEntry& pe = t.pose()[e0 + el];
-        V3 v, om;
-        column_twist(t, S, base, c, pe.link, v, om);
-        float* J = w.Jc() + (3 * el) * Dp + c;
-        if (pe.kind == kPosePosition) {
-            const Pose P = link_pose(t, Tj, base, pe.link);
-            const V3 pv = v + cross(om, V3{P.x, P.y, P.z});
-            J[0] = -pe.w[0] * pv.x;
-            J[Dp] = -pe.w[1] * pv.y;
-            J[2 * Dp] = -pe.w[2] * pv.z;
-        } else {
-            J[0] = pe.w[0] * om.x;
-            J[Dp] = pe.w[1] * om.y;
-            J[2 * Dp] = pe.w[2] * om.z;
+    const int D = t.h->D, Dp = t.h->Dp, boff = t.h->base_off;
+    for (int c = g.lane; c < D; c += G) {
+        bool single = false;
+        int j1 = 0;
+        V3 v1{0.f, 0.f, 0.f}, om1{0.f, 0.f, 0.f};
+        if (c >= boff) {
+            const int a = c - boff;
+            const int s0 = t.colstart()[a];
+            if (t.colstart()[a + 1] - s0 == 1) {
+                single = true;
+                j1 = t.coljoint()[s0];
+                const float m = t.colmul()[s0];
+                const float* sj = S + 8 * j1;
+                v1 = V3{0.f, 0.f, 0.f} + m * V3{sj[0], sj[1], sj[2]};
+                om1 = V3{0.f, 0.f, 0.f} + m * V3{sj[3], sj[4], sj[5]};
+            }
+        }
+        for (int el = 0; el < ne; ++el) {
+            const PoseEntry& pe = t.pose()[e0 + el];
+            V3 v, om;
+            if (single) {
+                const bool anc = (t.lanc()[pe.link] >> j1) & 1ull;
+                v = anc ? v1 : V3{0.f, 0.f, 0.f};
+                om = anc ? om1 : V3{0.f, 0.f, 0.f};
+            } else {
+                column_twist(t, S, base, c, pe.link, v, om);
+            }
+            float* J = w.Jc() + (3 * el) * Dp + c;
+            if (pe.kind == kPosePosition) {
+                const int jl = t.lpj()[pe.link];
+                const float* pp = jl >= 0 ? Tj + 8 * jl : base;
+                const V3 p = pp ? V3{pp[0], pp[1], pp[2]} : V3{0.f, 0.f, 0.f};
+                const V3 pv = v + cross(om, p);
+                J[0] = -pe.w[0] * pv.x;
+                J[Dp] = -pe.w[1] * pv.y;
+                J[2 * Dp] = -pe.w[2] * pv.z;
+            } else {
+                J[0] = pe.w[0] * om.x;
+                J[Dp] = pe.w[1] * om.y;
+                J[2 * Dp] = pe.w[2] * om.z;
+            }
         }
     }
     for (int r = g.lane; r < 3 * ne; r += G) w.Jc()[r * Dp + D] = w.rpose()[3 * e0 + r];
