@@ -1,0 +1,87 @@
+"""Host logic of the population solver, the IK helper and the serving stream (no GPU)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from robokit_b200 import _native as N
+from robokit_b200.helpers.ik import IKContext, IKSolverConfig, presets
+from robokit_b200.opt import LMOptimizerConfig
+from robokit_b200.opt.population_solver import PopulationSolverConfig, Stage
+from robokit_b200.opt.sampler import RobertsSampler, roberts_samples
+from robokit_b200.terms.task import Context
+
+
+def test_roberts_sequence():
+    """R_d: alpha_i = 1 - phi_d^-(i+1) with phi_d the root of x^(d+1) = x + 1 (d = 1: the golden ratio)."""
+    s = roberts_samples(6, 1)
+    phi = (1 + 5 ** 0.5) / 2
+    np.testing.assert_allclose(s[:, 0], np.modf(np.arange(6) * (1 - 1 / phi))[0], atol=1e-12)
+    s3 = roberts_samples(64, 3)
+    assert s3.shape == (64, 3) and s3.min() >= 0 and s3.max() < 1
+    phi3 = 1.0
+    for _ in range(60):
+        phi3 -= (phi3 ** 4 - phi3 - 1) / (4 * phi3 ** 3 - 1)
+    np.testing.assert_allclose(s3[1], 1 - phi3 ** -np.arange(1.0, 4.0), atol=1e-9)
+    # low discrepancy: every tenth of [0, 1) gets 4 to 8 of 64 points per axis (i.i.d. uniform draws spread wider)
+    counts = np.stack([np.histogram(s3[:, k], bins=10, range=(0, 1))[0] for k in range(3)])
+    assert counts.min() >= 4 and counts.max() <= 8
+
+
+def test_roberts_sampler_keep_first_and_tiling():
+    s = RobertsSampler(4, 2, keep_first=True)
+    assert np.all(s.offsets[0] == 0) and np.all(s.offsets[1] == -0.5)
+    t = s.tangent(3, np.array([2.0, 1.0], np.float32))
+    assert t.shape == (12, 2)
+    np.testing.assert_array_equal(t[4:8], t[0:4])
+    np.testing.assert_allclose(t[:4], s.offsets * [2.0, 1.0])
+    assert np.abs(t).max() <= 1.0
+
+
+def test_stage_resolution():
+    cfg = PopulationSolverConfig(stages=[Stage(6, 64, LMOptimizerConfig(lm_lambda=10.0)), Stage(10, 4), Stage(0, 1)])
+    assert cfg.num_candidates == [64, 4, 1]
+    assert [o.lm_lambda for o in cfg.optimizers] == [10.0, 10.0, 10.0]
+    assert presets.basic.solver.num_candidates == [64, 4, 1]
+    assert [o.lm_lambda for o in presets.basic.solver.optimizers] == [10.0, 1.0, 1.0]
+    assert presets.single_candidate.solver.num_candidates == [1]
+
+
+def test_ik_config_templates_and_validation():
+    assert isinstance(IKContext.TARGET, Context) and isinstance(IKContext.TARGET_LINKS, Context)
+    t = presets.basic.terms[0]
+    assert t.frame_index_arg is IKContext.TARGET_LINKS and t.weight == 20.0
+    with pytest.raises(ValueError, match="base_active_mask"):
+        IKSolverConfig(base_active_mask=(1, 1, 1, 0, 1, 1))
+    with pytest.raises(ValueError, match="length"):
+        IKSolverConfig(base_active_mask=(1, 1))
+
+
+def test_mixed_stream_shape():
+    from robokit_b200 import serve
+
+    class _Cfg:  # a stand-in pool: only the size is read
+        batch = 4096
+
+    types = [serve.StreamType(str(k), _Cfg(), None) for k in range(4)]
+    reqs = serve.make_stream(types, rate=100000.0, duration=2.0, seed=3)
+    assert reqs == serve.make_stream(types, rate=100000.0, duration=2.0, seed=3)  # seeded
+    t = np.array([r.t_arrive for r in reqs])
+    b = np.array([r.batch for r in reqs])
+    assert np.all(np.diff(t) > 0) and t[-1] < 2.0
+    assert b.min() >= 1 and b.max() <= 4096
+    assert all(0 <= r.start and r.start + r.batch <= 4096 for r in reqs)
+    # the problem rate is the requested one within sampling noise
+    assert 0.7 < b.sum() / 2.0 / 100000.0 < 1.4
+    assert {r.type_id for r in reqs} == {0, 1, 2, 3}
+
+
+def test_select_and_graph_argument_checks_need_no_device():
+    lib = N.load_library()
+    assert lib.ik_select_best(4, 8, 9, None, None, None, 3, None, None, None, None, None) == N.IK_E_INVALID
+    assert lib.ik_select_best(4, 8, 2, None, None, None, 3, None, None, None, None, None) == N.IK_E_INVALID
+    assert lib.ik_graph_begin(None) == N.IK_E_INVALID
+    assert lib.ik_graph_launch(None, None) == N.IK_E_INVALID
+    assert lib.ik_graph_destroy(None) == N.IK_OK
+    assert lib.ik_server_poll(None, None, 0, None) == N.IK_E_INVALID
