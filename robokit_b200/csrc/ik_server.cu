@@ -54,6 +54,8 @@ struct ServerCtrl {
     int* status;            // mapped [slots]
     const int* req_size;    // mapped [slots]: problems of each request
     int* req_count;         // device [slots]: problems finished so far
+    unsigned long long* req_ns;   // device [slots]: summed lane-group time of the request's problems
+    unsigned long long* req_ns_out;  // mapped [slots]: the same, published with the done flag
     int* req_flag;          // mapped [slots]: 1 when the request is complete
     const int* stop;        // mapped: 1 asks idle warps to exit
     int* quit_gen;          // device: highest launch generation that stopped claiming
@@ -61,6 +63,8 @@ struct ServerCtrl {
     int* host_head;         // mapped: the head as last claimed, for the host
     int gen;                // generation of this launch
     long long idle_ns;      // idle time after which the launch stops claiming
+    long long slice_ns;     // running time after which the launch stops claiming (the host relaunches
+                            // with rebalanced shares); 0 = no limit
 };
 
 __device__ __forceinline__ int ld_acquire_sys(const int* p) {
@@ -109,19 +113,33 @@ __device__ __forceinline__ void load_request_point(const Group<G>& g, const Tabs
 
 template <int G>
 __device__ __forceinline__ void finish_request_problem(const Group<G>& g, const Tabs& t, const Ws& w,
-                                                       const LmState& st, int slot, int req, const ServerCtrl& c) {
+                                                       const LmState& st, int slot, int req, const ServerCtrl& c,
+                                                       long long busy_ns) {
     store_solution<G>(g, t, w, st, slot, c.q_out, c.base_out, c.cost, c.lambda, c.iters, c.status);
     __threadfence_system();
     g.sync();
     if (g.lane == 0) {
+        atomicAdd(c.req_ns + req, (unsigned long long)(busy_ns > 0 ? busy_ns : 0));
+        __threadfence();
         const int done = atomicAdd(c.req_count + req, 1) + 1;
         if (done == __ldcv(c.req_size + req)) {
-            // the last problem of the request: no further increments on this counter
+            // the last problem of the request: no further increments on these counters
+            __threadfence();
+            c.req_ns_out[req] = atomicExch(c.req_ns + req, 0ull);
             c.req_count[req] = 0;
             __threadfence_system();
             *reinterpret_cast<volatile int*>(c.req_flag + req) = 1;
         }
     }
+}
+
+// This generation stops claiming: later tickets go to a new launch.
+__device__ __forceinline__ void stop_generation(const ServerCtrl& c) {
+    atomicMax(c.quit_gen, c.gen);
+    __threadfence();
+    *reinterpret_cast<volatile int*>(c.host_head) = *reinterpret_cast<volatile int*>(c.head);
+    __threadfence_system();
+    *reinterpret_cast<volatile int*>(c.host_quit) = c.gen;
 }
 
 // The serving form of the persistent kernel: lane groups own one problem at a
@@ -145,13 +163,23 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
     bool fresh = false;
     LmState st;
     long long idle_since = __shfl_sync(full, global_ns(), 0);
+    const long long t_launch = idle_since;
+    long long t_problem = 0;
     while (true) {
         const unsigned need = __ballot_sync(full, slot < 0 && g.lane == 0);
         int got = 0;
         if (need) {
             int hd = 0, k = 0;
-            if (lane == 0 && *reinterpret_cast<volatile int*>(c.quit_gen) < c.gen &&
-                *reinterpret_cast<const volatile int*>(c.stop) == 0) {
+            bool may_claim = false;
+            if (lane == 0) {
+                may_claim = *reinterpret_cast<volatile int*>(c.quit_gen) < c.gen &&
+                            *reinterpret_cast<const volatile int*>(c.stop) == 0;
+                if (may_claim && c.slice_ns > 0 && global_ns() - t_launch > c.slice_ns) {
+                    stop_generation(c);
+                    may_claim = false;
+                }
+            }
+            if (lane == 0 && may_claim) {
                 const int want = __popc(need);
                 hd = *reinterpret_cast<volatile int*>(c.head);
                 int tl = *reinterpret_cast<volatile int*>(c.mirror);
@@ -184,6 +212,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
                         slot = es;
                         req = er;
                         fresh = true;
+                        t_problem = global_ns();
                         load_request_point<G>(g, t, w, slot, c);
                         g.sync();
                     }
@@ -205,11 +234,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
                        *reinterpret_cast<const volatile int*>(c.stop) != 0;
                 if (!quit && global_ns() - idle_since > c.idle_ns &&
                     refresh_tail(c, true) <= *reinterpret_cast<volatile int*>(c.head)) {
-                    atomicMax(c.quit_gen, c.gen);
-                    __threadfence();
-                    *reinterpret_cast<volatile int*>(c.host_head) = *reinterpret_cast<volatile int*>(c.head);
-                    __threadfence_system();
-                    *reinterpret_cast<volatile int*>(c.host_quit) = c.gen;
+                    stop_generation(c);
                     quit = 1;
                 }
             }
@@ -223,7 +248,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_server_kernel(const char*
             if (fresh) stop = start_stops<G>(st, P);
             fresh = false;
             if (stop) {
-                finish_request_problem<G>(g, t, w, st, slot, req, c);
+                finish_request_problem<G>(g, t, w, st, slot, req, c, global_ns() - t_problem);
                 g.sync();
                 w.bind(group_ws<G>(wsbase, h, gib), h);
                 slot = -1;
@@ -292,6 +317,9 @@ struct ServerType {
     char* d_blob = nullptr;
     int* d_state = nullptr;          // [0] head, [1] tail mirror, [2..3] last poll time, [4] quit generation,
                                      // [8..] request counters
+    unsigned long long* d_req_ns = nullptr;  // [slots] summed problem times of running requests
+    Mapped req_ns_out;
+    double ns_per_problem = 0.0;     // running estimate of one problem's lane-group time (0 = none yet)
     Mapped q_in, base_in, q_out, base_out, cost, lambda, iters, status, ring, req_size, req_flag, tail;
     std::vector<Mapped> targets;     // one slab per pose term
     // generations rotate over kStreams streams, so a new launch can start
@@ -340,6 +368,7 @@ struct ServerType {
 struct IkServer {
     int64_t budget = 0, used = 0;
     long long idle_ns = 200000;
+    long long slice_ns = 4000000;  // generations rebalance the GPU share at least this often under load
     int stop_flag_set = 0;
     Mapped stop;
     std::vector<ServerType*> types;
@@ -367,6 +396,9 @@ int launch_type(IkServer* S, ServerType& T) {
     c.status = T.status.d<int>();
     c.req_size = T.req_size.d<int>();
     c.req_count = T.d_state + kStateHeader;
+    c.req_ns = T.d_req_ns;
+    c.req_ns_out = T.req_ns_out.d<unsigned long long>();
+    c.slice_ns = S->slice_ns;
     c.req_flag = T.req_flag.d<int>();
     c.stop = S->stop.d<int>();
     c.quit_gen = T.d_state + 4;
@@ -375,13 +407,26 @@ int launch_type(IkServer* S, ServerType& T) {
     c.gen = T.gen + 1;
     const int sidx = c.gen % kStreams;
     c.idle_ns = S->idle_ns;
-    // share the GPU between the kernels of the types with work, so that all of them stay resident
+    // Share the GPU between the kernels of the types with work, so that all of them stay resident: by
+    // their waiting work in block-time (waiting problems x measured time per problem / groups per block)
+    // once every such type has a measurement, else evenly.
+    double total = 0.0, mine = 0.0;
     int ntypes = 0;
-    for (ServerType* o : S->types) ntypes += (o == &T || !o->inflight.empty()) ? 1 : 0;
+    bool measured = true;
+    for (ServerType* o : S->types) {
+        if (o != &T && o->inflight.empty()) continue;
+        ++ntypes;
+        const int waiting = std::max(1, o->tail_host - __atomic_load_n(o->tail.h<int>() + kHostHead, __ATOMIC_ACQUIRE));
+        const double d = waiting * o->ns_per_problem / (kBlockThreads / o->G);
+        if (o->ns_per_problem <= 0.0) measured = false;
+        total += d;
+        if (o == &T) mine = d;
+    }
     ntypes = std::max(ntypes, 1);
+    const double share = (measured && total > 0.0) ? std::max(mine / total, 0.02) : 1.0 / ntypes;
     const int gpb = kBlockThreads / T.G;
     const int need = (T.slots + gpb - 1) / gpb;
-    int grid = std::max(1, T.per_sm * num_sms() / ntypes);
+    int grid = std::max(1, (int)(T.per_sm * num_sms() * share + 0.5));
     grid = std::min(grid, need);
     // types of the same group width share a kernel: set its shared-memory limit for this type
     int rc = IK_OK;
@@ -458,8 +503,9 @@ void release_type(ServerType* T) {
     for (int k = 0; k < kStreams; ++k)
         if (T->stream[k]) cudaStreamSynchronize(T->stream[k]);
     for (Mapped* m : {&T->q_in, &T->base_in, &T->q_out, &T->base_out, &T->cost, &T->lambda, &T->iters, &T->status,
-                      &T->ring, &T->req_size, &T->req_flag, &T->tail})
+                      &T->ring, &T->req_size, &T->req_flag, &T->tail, &T->req_ns_out})
         m->release();
+    if (T->d_req_ns) cudaFree(T->d_req_ns);
     for (auto& m : T->targets) m.release();
     if (T->d_blob) cudaFree(T->d_blob);
     if (T->d_state) cudaFree(T->d_state);
@@ -549,6 +595,7 @@ int ik_server_add_type(IkServer* S, IkRobot* robot, int32_t floating_base, const
     if (!rc) rc = take(T->req_size, ns * 4);
     if (!rc) rc = take(T->req_flag, ns * 4);
     if (!rc) rc = take(T->tail, 256);
+    if (!rc) rc = take(T->req_ns_out, ns * 8);
     T->targets.resize(T->pose_terms.size());
     for (size_t k = 0; k < T->pose_terms.size() && !rc; ++k) {
         rc = take(T->targets[k], ns * T->pose_frames[k] * 7 * 4);
@@ -578,12 +625,14 @@ int ik_server_add_type(IkServer* S, IkRobot* robot, int32_t floating_base, const
             e = cudaMemcpy(T->d_blob, T->tab.blob.data(), T->tab.blob.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMalloc(&T->d_state, (ns + kStateHeader) * sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(T->d_state, 0, (ns + kStateHeader) * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&T->d_req_ns, ns * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemset(T->d_req_ns, 0, ns * sizeof(unsigned long long));
         for (int k = 0; k < kStreams; ++k) {
             if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&T->stream[k], cudaStreamNonBlocking);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&T->done_ev[k], cudaEventDisableTiming);
         }
         if (e != cudaSuccess) rc = fail(IK_E_OOM, "server type buffers: %s", cudaGetErrorString(e));
-        bytes += (int64_t)T->tab.blob.size() + (int64_t)(ns + kStateHeader) * 4;
+        bytes += (int64_t)T->tab.blob.size() + (int64_t)(ns + kStateHeader) * 4 + (int64_t)ns * 8;
     }
     if (!rc) {
         int per_sm = 0;
@@ -658,6 +707,8 @@ int ik_server_poll(IkServer* S, int64_t* done_ids, int32_t max_done, int32_t* nu
             if (__atomic_load_n(T.req_flag.h<int>() + R.req, __ATOMIC_ACQUIRE) == 1 &&
                 (done_ids == nullptr || n < max_done)) {
                 R.done = true;
+                const double per = (double)T.req_ns_out.h<unsigned long long>()[R.req] / R.batch;
+                T.ns_per_problem = T.ns_per_problem > 0.0 ? 0.8 * T.ns_per_problem + 0.2 * per : per;
                 if (done_ids) done_ids[n] = R.id;
                 ++n;
                 T.inflight[i] = T.inflight.back();
