@@ -58,6 +58,8 @@ extern "C" {
 #define IK_TERM_ROTATION 2       /* terms/dense/rotation_task.py:25            */
 #define IK_TERM_POSITION_LIMIT 3 /* terms/dense/position_limit.py:185 ("abs")  */
 #define IK_TERM_SELF_COLLISION 4 /* terms/dense/self_collision_task.py:593     */
+#define IK_TERM_FRAME 5          /* terms/dense/frame_task.py:47 ("log" mode): six rows per frame,
+                                    weights [num_frames*2] = (position, orientation) per frame */
 
 /* self-collision pair modes */
 #define IK_PAIRS_SLOTS 0 /* reference: <= K link pairs, most penetrating sphere pair each */

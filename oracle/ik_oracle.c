@@ -143,6 +143,101 @@ static void quat_axis_angle(const double* q, double* o) {
     for (int k = 0; k < 3; ++k) o[k] = q[1 + k] / s;
 }
 
+/* 3x3 helpers, row-major */
+static void m3_hat(const double* a, double* H) {
+    H[0] = 0.0; H[1] = -a[2]; H[2] = a[1];
+    H[3] = a[2]; H[4] = 0.0; H[5] = -a[0];
+    H[6] = -a[1]; H[7] = a[0]; H[8] = 0.0;
+}
+static void m3_mul(const double* A, const double* B, double* C) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+static void m3_quat(const double* q, double* R) {
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    R[0] = 1 - 2 * (y * y + z * z); R[1] = 2 * (x * y - w * z); R[2] = 2 * (x * z + w * y);
+    R[3] = 2 * (x * y + w * z); R[4] = 1 - 2 * (x * x + z * z); R[5] = 2 * (y * z - w * x);
+    R[6] = 2 * (x * z - w * y); R[7] = 2 * (y * z + w * x); R[8] = 1 - 2 * (x * x + y * y);
+}
+
+/* SE(3) logarithm [V^-1(w) t; w], V^-1 = I - W/2 + c2 W^2 (se3_log_map_func and
+ * se3_V_matrix_inverse_func, lie/se3_kernels.py:230-311; eps 1e-4 as frame_task.py:523) */
+static void se3_log6(const P7* E, double* out) {
+    double w[3];
+    quat_axis_angle(E->q, w);
+    const double th = sqrt(dot3(w, w));
+    double c2 = 1.0 / 12.0;
+    if (!(th < 1e-4)) {
+        const double omc = 1.0 - cos(th);
+        if (!(fabs(omc) < 1e-4)) c2 = (1.0 / (th * th)) * (1.0 - (th * sin(th)) / (2.0 * omc));
+    }
+    double wt[3], wwt[3];
+    cross3(w, E->t, wt);
+    cross3(w, wt, wwt);
+    for (int k = 0; k < 3; ++k) {
+        out[k] = E->t[k] - 0.5 * wt[k] + c2 * wwt[k];
+        out[3 + k] = w[k];
+    }
+}
+
+/* 6x6 SE(3) jlog (se3_jlog_func, lie/se3_kernels.py:359-428, with so3_jac_left_inv_func,
+ * lie/so3_kernels.py:14-40): [[A, B], [0, A]], A = Jl^-1(w)^T; eps 1e-4 on |w|^2 */
+static void se3_jlog6(const P7* F, double* M) {
+    double w[3], W[9], W2[9], A[9], B[9], Hp[9];
+    quat_axis_angle(F->q, w);
+    const double th2 = dot3(w, w);
+    const int taylor = th2 < 1e-4;
+    m3_hat(w, W);
+    m3_mul(W, W, W2);
+    double coeff = 1.0 / 12.0, th = 1.0;
+    if (!taylor) {
+        th = sqrt(th2);
+        coeff = (1.0 - th * cos(0.5 * th) / (2.0 * sin(0.5 * th))) / th2;
+    }
+    for (int k = 0; k < 9; ++k) A[k] = ((k % 4) == 0 ? 1.0 : 0.0) + 0.5 * W[k] + coeff * W2[k];
+    m3_hat(F->t, Hp);
+    if (taylor) {
+        for (int k = 0; k < 9; ++k) B[k] = 0.5 * Hp[k];
+    } else {
+        const double st = sin(th), ct = cos(th), inv = 1.0 / th, inv2 = inv * inv;
+        const double i22 = 1.0 / (2.0 * (1.0 - ct));
+        const double beta = inv2 - st * inv * i22;
+        const double bdot = -2.0 * inv2 * inv2 + (1.0 + st * inv) * inv2 * i22;
+        const double wtp = dot3(w, F->t);
+        double C[9];
+        for (int i = 0; i < 3; ++i) {
+            const double v3 = bdot * wtp * w[i] - (th2 * bdot + 2.0 * beta) * F->t[i];
+            for (int j = 0; j < 3; ++j)
+                C[3 * i + j] = v3 * w[j] + beta * w[i] * F->t[j] + (i == j ? wtp * beta : 0.0) + 0.5 * Hp[3 * i + j];
+        }
+        m3_mul(C, A, B);
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            double v = 0.0;
+            if (i < 3 && j < 3) v = A[3 * i + j];
+            else if (i < 3) v = B[3 * i + j - 3];
+            else if (j >= 3) v = A[3 * (i - 3) + j - 3];
+            M[6 * i + j] = v;
+        }
+}
+
+/* 6x6 adjoint [[R, hat(t) R], [0, R]] (se3_adjoint_func, lie/se3_kernels.py:314-346) */
+static void se3_adjoint6(const P7* T, double* M) {
+    double R[9], H[9], HR[9];
+    m3_quat(T->q, R);
+    m3_hat(T->t, H);
+    m3_mul(H, R, HR);
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            double v = 0.0;
+            if (i < 3 && j < 3) v = R[3 * i + j];
+            else if (i < 3) v = HR[3 * i + j - 3];
+            else if (j >= 3) v = R[3 * (i - 3) + j - 3];
+            M[6 * i + j] = v;
+        }
+}
+
 /* ------------------------------------------------------------------------ */
 /* per-problem kinematic state                                               */
 /* ------------------------------------------------------------------------ */
@@ -332,6 +427,8 @@ int or_residual_dim(const OrRobot* r, const OrTerm* terms, int32_t nterms) {
         const OrTerm* t = terms + i;
         if (t->kind == 1 || t->kind == 2)
             R += 3 * t->num_frames;
+        else if (t->kind == 5)
+            R += 6 * t->num_frames;
         else if (t->kind == 3)
             R += r->na;
         else if (t->kind == 4)
@@ -404,6 +501,52 @@ static void eval_terms(const OrRobot* r, const OrTerm* terms, int nterms, int fl
                 }
             }
             row += 3 * t->num_frames;
+        } else if (t->kind == 5) {
+            /* frame_task.py:391-527 ("log"): r = w (.) log(T_frame^-1 T_target);
+             * J column = -w (.) jlog(T_target^-1 T_frame) Ad(T_frame^-1) [v; om] */
+            for (int f = 0; f < t->num_frames; ++f) {
+                const P7 P = link_pose(r, K, t->frame_links[f]);
+                const P7 T = p7_from_f(term_target(t, b, B, f));
+                const double wp = t->weights[2 * f], wr = t->weights[2 * f + 1];
+                const P7 Pi = inverse(&P);
+                const P7 E = compose(&Pi, &T);
+                double lg[6];
+                se3_log6(&E, lg);
+                const double pe = sqrt(dot3(E.t, E.t));
+                if (pe > mp) mp = pe;
+                double sn = sqrt(E.q[1] * E.q[1] + E.q[2] * E.q[2] + E.q[3] * E.q[3]);
+                if (sn > 1.0) sn = 1.0;
+                const double ang = 2.0 * asin(sn);
+                if (ang > mr) mr = ang;
+                for (int k = 0; k < 6; ++k) res[row + 6 * f + k] = (k < 3 ? wp : wr) * lg[k];
+                if (J) {
+                    const P7 Ti = inverse(&T);
+                    const P7 F = compose(&Ti, &P);
+                    double M1[36], M2[36], M[36];
+                    se3_jlog6(&F, M1);
+                    se3_adjoint6(&Pi, M2);
+                    for (int i = 0; i < 6; ++i)
+                        for (int j = 0; j < 6; ++j) {
+                            double v = 0.0;
+                            for (int k = 0; k < 6; ++k) v += M1[6 * i + k] * M2[6 * k + j];
+                            M[6 * i + j] = v;
+                        }
+                    for (int c = 0; c < D; ++c) {
+                        double v[3], om[3], s6[6];
+                        column_twist(r, K, floating, c, t->frame_links[f], v, om);
+                        for (int k = 0; k < 3; ++k) {
+                            s6[k] = v[k];
+                            s6[3 + k] = om[k];
+                        }
+                        for (int i = 0; i < 6; ++i) {
+                            double col = 0.0;
+                            for (int k = 0; k < 6; ++k) col += M[6 * i + k] * s6[k];
+                            J[(size_t)(row + 6 * f + i) * D + c] = -(i < 3 ? wp : wr) * col;
+                        }
+                    }
+                }
+            }
+            row += 6 * t->num_frames;
         } else if (t->kind == 3) {
             /* position_limit.py:509-573 ("abs") */
             for (int a = 0; a < r->na; ++a) {

@@ -35,7 +35,7 @@ typedef struct OrRobot {
 } OrRobot;
 
 typedef struct OrTerm {
-    int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision */
+    int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision, 5 frame ("log") */
     int32_t num_frames;
     const int32_t* frame_links;
     const float* weights;

@@ -35,6 +35,7 @@ IK_TERM_POSITION = 1
 IK_TERM_ROTATION = 2
 IK_TERM_POSITION_LIMIT = 3
 IK_TERM_SELF_COLLISION = 4
+IK_TERM_FRAME = 5
 
 IK_PAIRS_SLOTS = 0
 IK_PAIRS_ALL = 1

@@ -128,7 +128,8 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_sph = take(need_sph ? ns * 16 : 0);
     h->w_lbw = take(need_lbw ? nl * 16 : 0);
     h->w_tgt = take(npose * 8 * 4);
-    h->w_rpose = take(npose * 3 * 4);
+    h->w_rpose = take(std::max(h->pose_rows, 3 * npose) * 4);
+    h->w_fM = take(h->nframe * 18 * 4);
     h->w_rlim = take(na * 4);
     // The Jacobian chunk and its row records live only inside a linearisation and
     // the FP64 factor only inside a solve: they share one region.
@@ -231,6 +232,9 @@ int check_launch() {
         g_launches.fetch_add(1);
     return IK_OK;
 }
+
+template <int G>
+constexpr auto lm_persistent_noframe = lm_persistent_kernel<G, false>;
 
 // Dispatch a templated kernel on the group width.
 #define IK_DISPATCH(G, KERNEL, ...)                                   \
@@ -536,23 +540,32 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     std::vector<PoseEntry> pose;
     std::vector<CollEntry> coll;
     std::vector<float> limw(std::max(r.na, 1), 0.f);
-    int has_limit = 0, limit_row = 0;
+    int has_limit = 0, limit_row = 0, pose_rows = 0, nframe = 0;
     for (size_t ti = 0; ti < terms.size(); ++ti) {
         const TermHost& th = terms[ti];
         const int kind = th.d.kind;
-        if (kind == IK_TERM_POSITION || kind == IK_TERM_ROTATION) {
+        if (kind == IK_TERM_POSITION || kind == IK_TERM_ROTATION || kind == IK_TERM_FRAME) {
+            const bool frame = kind == IK_TERM_FRAME;
             for (int f = 0; f < th.d.num_frames; ++f) {
                 PoseEntry e;
                 std::memset(&e, 0, sizeof(e));
                 e.link = th.frame_links[f];
-                e.kind = kind == IK_TERM_POSITION ? kPosePosition : kPoseRotation;
+                e.kind = frame ? kPoseFrame : (kind == IK_TERM_POSITION ? kPosePosition : kPoseRotation);
                 e.term = (int)ti;
                 e.frame = f;
                 e.num_frames = th.d.num_frames;
-                e.out_row = th.row + 3 * f;
+                e.out_row = th.row + (frame ? 6 : 3) * f;
                 e.target_rows = th.d.target_rows;
-                for (int k = 0; k < 3; ++k) e.w[k] = th.weights[3 * f + k];
+                e.r0 = pose_rows;
+                e.fm = frame ? nframe++ : -1;
+                if (frame) {
+                    e.w[0] = th.weights[2 * f];
+                    e.w[1] = th.weights[2 * f + 1];
+                } else {
+                    for (int k = 0; k < 3; ++k) e.w[k] = th.weights[3 * f + k];
+                }
                 e.targets = th.d.d_targets;
+                pose_rows += frame ? 6 : 3;
                 pose.push_back(e);
             }
         } else if (kind == IK_TERM_POSITION_LIMIT) {
@@ -563,6 +576,8 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     }
     h = b.hdr();
     h->npose = (int)pose.size();
+    h->pose_rows = pose_rows;
+    h->nframe = nframe;
     h->has_limit = has_limit;
     h->limit_row = limit_row;
     // collision arrays
@@ -631,7 +646,7 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         h->t_qp = take(std::max(h->na, 1));
         h->t_base = take(h->base_off ? 7 : 0);
         h->t_basep = take(h->base_off ? 7 : 0);
-        bool ok = h->D <= kSmallD;
+        bool ok = h->D <= kSmallD && h->nframe == 0;
         for (size_t i = 0; i < coll.size(); ++i) {
             if (ce[i].mode != IK_PAIRS_ALL) ok = false;
             ce[i].t_mask = take((ce[i].nsp + 31) / 32);
@@ -660,7 +675,7 @@ int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc*
         TermHost th;
         th.d = d;
         th.row = row;
-        if (d.kind == IK_TERM_POSITION || d.kind == IK_TERM_ROTATION) {
+        if (d.kind == IK_TERM_POSITION || d.kind == IK_TERM_ROTATION || d.kind == IK_TERM_FRAME) {
             if (d.num_frames < 1 || !d.frame_links || !d.weights) {
                 return fail(IK_E_INVALID, "term %d: pose term needs frames and weights", i);
             }
@@ -672,8 +687,9 @@ int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc*
                 if (f < 0 || f >= r.nl) {
                         return fail(IK_E_INVALID, "term %d: frame link %d out of range", i, f);
                 }
-            th.weights.assign(d.weights, d.weights + 3 * d.num_frames);
-            th.rows = 3 * d.num_frames;
+            const int per = d.kind == IK_TERM_FRAME ? 2 : 3;
+            th.weights.assign(d.weights, d.weights + per * d.num_frames);
+            th.rows = (d.kind == IK_TERM_FRAME ? 6 : 3) * d.num_frames;
         } else if (d.kind == IK_TERM_POSITION_LIMIT) {
             if (++nlimit > 1) {
                 return fail(IK_E_UNSUPPORTED, "more than one PositionLimit term");
@@ -875,7 +891,7 @@ int ik_problem_set_targets(IkProblem* P, int32_t term_index, const float* d_targ
     if (!P) return fail(IK_E_INVALID, "problem is NULL");
     if (term_index < 0 || term_index >= (int)P->terms.size()) return fail(IK_E_INVALID, "term %d out of range", term_index);
     TermHost& th = P->terms[term_index];
-    if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION)
+    if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION && th.d.kind != IK_TERM_FRAME)
         return fail(IK_E_INVALID, "term %d has no pose targets", term_index);
     if (!d_targets) return fail(IK_E_INVALID, "targets are NULL");
     th.d.d_targets = d_targets;
@@ -979,6 +995,21 @@ int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, 
     }
     const int G = problem_group(P);
     const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
+    if (reinterpret_cast<const TabHeader*>(P->blob.data())->nframe == 0) {
+        // no frame entries: the kernel without the frame paths (a smaller instruction footprint)
+        IK_DISPATCH(G, lm_persistent_noframe, {
+            rc = prepare_kernel(kfn, smem);
+            if (rc) return rc;
+            int grid = 0;
+            rc = grid_for(kfn, smem, batch, G, P->blocks_per_sm, grid, kBlockThreads);
+            if (rc) return rc;
+            kfn<<<grid, kBlockThreads, smem, S(stream)>>>(P->d_blob, batch, d_q, d_base, prm, P->d_queue, d_cost,
+                                                          d_lambda, d_iters, d_status);
+            rc = check_launch();
+            if (rc) return rc;
+        });
+        return IK_OK;
+    }
     IK_DISPATCH(G, lm_persistent_kernel, {
         rc = prepare_kernel(kfn, smem);
         if (rc) return rc;

@@ -136,6 +136,124 @@ __device__ __forceinline__ V3 quat_to_axis_angle(float w, float i, float j, floa
     return V3{i * inv_s, j * inv_s, k * inv_s};
 }
 
+// T^-1 with the conjugate quaternion, se3_inverse_func (lie/se3_kernels.py:70-78)
+__device__ __forceinline__ Pose pose_inverse(const Pose& T) {
+    const V3 ti = qrot(T.w, -T.i, -T.j, -T.k, V3{T.x, T.y, T.z});
+    return Pose{-ti.x, -ti.y, -ti.z, T.w, -T.i, -T.j, -T.k};
+}
+
+// SE(3) logarithm [V^-1(w) t; w] with V^-1 = I - W/2 + c2 W^2, W = hat(w)
+// (se3_log_map_func, lie/se3_kernels.py:230-311; eps 1e-4 as frame_task.py:523)
+__device__ __forceinline__ void se3_log(const Pose& E, float out[6], float& angle) {
+    const V3 w = quat_to_axis_angle(E.w, E.i, E.j, E.k, angle);
+    const float th = norm3(w);
+    float c2 = 1.0f / 12.0f;
+    if (!(th < 1e-4f)) {
+        float sn, cs;
+        sincosf(th, &sn, &cs);
+        const float omc = 1.0f - cs;
+        if (!(fabsf(omc) < 1e-4f)) c2 = (1.0f / (th * th)) * (1.0f - (th * sn) / (2.0f * omc));
+    }
+    const V3 t{E.x, E.y, E.z};
+    const V3 wt = cross(w, t);
+    const V3 wwt = cross(w, wt);
+    out[0] = t.x - 0.5f * wt.x + c2 * wwt.x;
+    out[1] = t.y - 0.5f * wt.y + c2 * wwt.y;
+    out[2] = t.z - 0.5f * wt.z + c2 * wwt.z;
+    out[3] = w.x;
+    out[4] = w.y;
+    out[5] = w.z;
+}
+
+// Six weighted rows w (.) log(T_frame^-1 T_target) of a frame entry into rp, folded into the
+// compensated cost and the pose errors (frame_task.py:505-527).  Out of line: frame entries are
+// rare, and the solve loops keep their instruction footprint without them.
+__device__ __forceinline__ void frame_residual(const Pose& P, const float* tg, float wp, float wr, float* rp, float& ks,
+                                            float& kc, float& max_pos, float& max_rot);
+
+// 3x3 helpers, row-major
+__device__ __forceinline__ void m3_hat(const V3& a, float H[9]) {
+    H[0] = 0.f; H[1] = -a.z; H[2] = a.y;
+    H[3] = a.z; H[4] = 0.f; H[5] = -a.x;
+    H[6] = -a.y; H[7] = a.x; H[8] = 0.f;
+}
+__device__ __forceinline__ void m3_mul(const float A[9], const float B[9], float C[9]) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+__device__ __forceinline__ V3 m3_vec(const float A[9], const V3& v) {
+    return V3{A[0] * v.x + A[1] * v.y + A[2] * v.z, A[3] * v.x + A[4] * v.y + A[5] * v.z,
+              A[6] * v.x + A[7] * v.y + A[8] * v.z};
+}
+// rotation matrix of a unit quaternion (quaternion_to_matrix_func, rotation_conversions.py:169-183)
+__device__ __forceinline__ void m3_quat(float w, float x, float y, float z, float R[9]) {
+    R[0] = 1.f - 2.f * (y * y + z * z); R[1] = 2.f * (x * y - w * z); R[2] = 2.f * (x * z + w * y);
+    R[3] = 2.f * (x * y + w * z); R[4] = 1.f - 2.f * (x * x + z * z); R[5] = 2.f * (y * z - w * x);
+    R[6] = 2.f * (x * z - w * y); R[7] = 2.f * (y * z + w * x); R[8] = 1.f - 2.f * (x * x + y * y);
+}
+
+// Jacobian factors of a frame residual (frame_task.py:391-456): for a world twist [v; om] of a
+// tangent column the six rows are -w (.) [P v + K om; P om], where with F = T_target^-1 T_frame,
+// (w, p) its axis-angle and translation, A = Jl^-1(w)^T (so3_jac_left_inv_func,
+// lie/so3_kernels.py:14-40), B the upper-right block of the SE(3) jlog (se3_jlog_func,
+// lie/se3_kernels.py:359-428) and (t_i, R_i) = T_frame^-1 (se3_adjoint_func :314-346):
+//   P = A R_i,   K = (A hat(t_i) + B) R_i.
+__device__ __forceinline__ void frame_jacobian_factors(const Pose& Tf, const Pose& Tt, float P[9], float K[9]) {
+    const Pose F = compose(pose_inverse(Tt), Tf);
+    float ang;
+    const V3 w = quat_to_axis_angle(F.w, F.i, F.j, F.k, ang);
+    const V3 p{F.x, F.y, F.z};
+    const float th2 = dot(w, w);
+    const bool taylor = th2 < 1e-4f;
+    float W[9], W2[9], A[9], B[9];
+    m3_hat(w, W);
+    m3_mul(W, W, W2);
+    float coeff = 1.0f / 12.0f;
+    float th = 1.0f;
+    if (!taylor) {
+        th = sqrtf(th2);
+        float sh, ch;
+        sincosf(0.5f * th, &sh, &ch);
+        coeff = (1.0f - th * ch / (2.0f * sh)) / th2;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) A[k] = ((k % 4) == 0 ? 1.f : 0.f) + 0.5f * W[k] + coeff * W2[k];
+    float Hp[9];
+    m3_hat(p, Hp);
+    if (taylor) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) B[k] = 0.5f * Hp[k];
+    } else {
+        float st, ct;
+        sincosf(th, &st, &ct);
+        const float inv = 1.0f / th, inv2 = inv * inv;
+        const float i22 = 1.0f / (2.0f * (1.0f - ct));
+        const float beta = inv2 - st * inv * i22;
+        const float bdot = -2.0f * inv2 * inv2 + (1.0f + st * inv) * inv2 * i22;
+        const float wtp = dot(w, p);
+        const V3 v3 = (bdot * wtp) * w - (th2 * bdot + 2.0f * beta) * p;
+        const float vv[3] = {v3.x, v3.y, v3.z}, ww[3] = {w.x, w.y, w.z}, pp[3] = {p.x, p.y, p.z};
+        float C[9];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                C[3 * i + j] = vv[i] * ww[j] + beta * ww[i] * pp[j] + (i == j ? wtp * beta : 0.f) + 0.5f * Hp[3 * i + j];
+        m3_mul(C, A, B);
+    }
+    const Pose Ti = pose_inverse(Tf);
+    float R[9], Ht[9], AH[9];
+    m3_quat(Ti.w, Ti.i, Ti.j, Ti.k, R);
+    m3_hat(V3{Ti.x, Ti.y, Ti.z}, Ht);
+    m3_mul(A, R, P);
+    m3_mul(A, Ht, AH);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) AH[k] += B[k];
+    m3_mul(AH, R, K);
+}
+
 // ---------------------------------------------------------------------------
 // compensated accumulation (Neumaier's variant of Kahan summation)
 // ---------------------------------------------------------------------------
@@ -146,6 +264,21 @@ __device__ __forceinline__ void kadd(float& s, float& c, float x) {
     else
         c += (x - t) + s;
     s = t;
+}
+
+__device__ __forceinline__ void frame_residual(const Pose& P, const float* tg, float wp, float wr, float* rp, float& ks,
+                                            float& kc, float& max_pos, float& max_rot) {
+    const Pose E = compose(pose_inverse(P), Pose{tg[0], tg[1], tg[2], tg[3], tg[4], tg[5], tg[6]});
+    float lg[6], angle;
+    se3_log(E, lg, angle);
+    max_pos = fmaxf(max_pos, norm3(V3{E.x, E.y, E.z}));
+    max_rot = fmaxf(max_rot, angle);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float r = (k < 3 ? wp : wr) * lg[k];
+        rp[k] = r;
+        kadd(ks, kc, r * r);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -266,6 +399,7 @@ struct Ws {
     IK_WS(float, tgt, w_tgt)          // pose targets [npose*8]
     IK_WS(float, rpose, w_rpose)      // pose residuals [npose*3]
     IK_WS(float, rlim, w_rlim)        // limit residuals [na]
+    IK_WS(float, fM, w_fM)            // frame entries: Jacobian factors P, K [nframe*18]
     IK_WS(float, Jc, w_Jc)            // chunk rows [kChunkRows*Dp]: D Jacobian columns, then the residual
     IK_WS(float, rowmeta, w_rowmeta)  // chunk row records [kChunkRows*2]: sphere pair i | j << 16, residual
     IK_WS(float, Hs, w_Hs)            // normal equations [E] (packed lower H, then g)
@@ -532,7 +666,8 @@ struct EvalOut {
     int nslots;     // filled slots summed over slot-mode terms
 };
 
-template <int G>
+// F: the tables may hold frame entries (false compiles the frame paths out)
+template <int G, bool F = true>
 __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, Ws& w, const float* q, const float* base) {
     const TabHeader* h = t.h;
     EvalOut o;
@@ -564,6 +699,11 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
         const PoseEntry& pe = t.pose()[e];
         const Pose P = link_pose(t, Tj, base, pe.link);
         const float* tg = w.tgt() + 8 * e;
+        float* rp = w.rpose() + pe.r0;
+        if (F && pe.kind == kPoseFrame) {
+            frame_residual(P, tg, pe.w[0], pe.w[1], rp, ks, kc, max_pos, max_rot);
+            continue;
+        }
         V3 r;
         if (pe.kind == kPosePosition) {
             const V3 err{tg[0] - P.x, tg[1] - P.y, tg[2] - P.z};
@@ -577,9 +717,9 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
             max_rot = fmaxf(max_rot, angle);
             r = V3{pe.w[0] * aa.x, pe.w[1] * aa.y, pe.w[2] * aa.z};
         }
-        w.rpose()[3 * e] = r.x;
-        w.rpose()[3 * e + 1] = r.y;
-        w.rpose()[3 * e + 2] = r.z;
+        rp[0] = r.x;
+        rp[1] = r.y;
+        rp[2] = r.z;
         kadd(ks, kc, r.x * r.x);
         kadd(ks, kc, r.y * r.y);
         kadd(ks, kc, r.z * r.z);
@@ -767,14 +907,53 @@ __device__ __forceinline__ void group_accumulate_chunk(const Group<G>& g, const 
     g.sync();
 }
 
-// Build the Jacobian of pose entries [e0, e0+ne) into the chunk (3 rows each).
+__device__ __forceinline__ int pose_entry_rows(const PoseEntry& pe) { return pe.kind == kPoseFrame ? 6 : 3; }
+
+// The six Jacobian entries of a frame entry for one column with world twist [v; om].
+__device__ __forceinline__ void frame_rows(const float* f, V3 v, V3 om, float wp, float wr, float* J, int Dp) {
+    const V3 top = m3_vec(f, v) + m3_vec(f + 9, om);
+    const V3 bot = m3_vec(f, om);
+    J[0] = -wp * top.x;
+    J[Dp] = -wp * top.y;
+    J[2 * Dp] = -wp * top.z;
+    J[3 * Dp] = -wr * bot.x;
+    J[4 * Dp] = -wr * bot.y;
+    J[5 * Dp] = -wr * bot.z;
+}
+
+// Pose entries [e0, e1) whose rows fit one chunk, starting at e0.
+__device__ __forceinline__ int pose_chunk_end(const Tabs& t, int e0) {
+    const int npose = t.h->npose;
+    int e1 = e0, rows = 0;
+    while (e1 < npose && rows + pose_entry_rows(t.pose()[e1]) <= kChunkRows) rows += pose_entry_rows(t.pose()[e1++]);
+    return e1;
+}
+
+// Jacobian factors of every frame entry at the current point (see frame_jacobian_factors).
+template <int G, bool F = true>
+__device__ __forceinline__ void group_frame_factors(const Group<G>& g, const Tabs& t, Ws& w, const float* Tj,
+                                                    const float* base) {
+    if (!F || t.h->nframe == 0) return;
+    for (int e = g.lane; e < t.h->npose; e += G) {
+        const PoseEntry& pe = t.pose()[e];
+        if (pe.kind != kPoseFrame) continue;
+        const float* tg = w.tgt() + 8 * e;
+        float* f = w.fM() + 18 * pe.fm;
+        frame_jacobian_factors(link_pose(t, Tj, base, pe.link), Pose{tg[0], tg[1], tg[2], tg[3], tg[4], tg[5], tg[6]},
+                               f, f + 9);
+    }
+    g.sync();
+}
+
+// Build the Jacobian of pose entries [e0, e1) into the chunk (3 rows each, 6 for a frame entry).
 // A lane owns a tangent column and walks the entries: a column driven by one
 // joint (the usual case) loads that joint's twist once and only tests, per
 // entry, whether the joint is an ancestor of the entry's link.
-template <int G>
+template <int G, bool F = true>
 __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t, Ws& w, const float* Tj, const float* S,
-                                const float* base, int e0, int ne) {
+                                const float* base, int e0, int e1) {
     const int D = t.h->D, Dp = t.h->Dp, boff = t.h->base_off;
+    const int rbase = t.pose()[e0].r0;
     for (int c = g.lane; c < D; c += G) {
         bool single = false;
         int j1 = 0;
@@ -791,8 +970,8 @@ __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t
                 om1 = V3{0.f, 0.f, 0.f} + m * V3{sj[3], sj[4], sj[5]};
             }
         }
-        for (int el = 0; el < ne; ++el) {
-            const PoseEntry& pe = t.pose()[e0 + el];
+        for (int el = e0; el < e1; ++el) {
+            const PoseEntry& pe = t.pose()[el];
             V3 v, om;
             if (single) {
                 const bool anc = (t.lanc()[pe.link] >> j1) & 1ull;
@@ -801,8 +980,10 @@ __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t
             } else {
                 column_twist(t, S, base, c, pe.link, v, om);
             }
-            float* J = w.Jc() + (3 * el) * Dp + c;
-            if (pe.kind == kPosePosition) {
+            float* J = w.Jc() + (pe.r0 - rbase) * Dp + c;
+            if (F && pe.kind == kPoseFrame) {
+                frame_rows(w.fM() + 18 * pe.fm, v, om, pe.w[0], pe.w[1], J, Dp);
+            } else if (pe.kind == kPosePosition) {
                 const int jl = t.lpj()[pe.link];
                 const float* pp = jl >= 0 ? Tj + 8 * jl : base;
                 const V3 p = pp ? V3{pp[0], pp[1], pp[2]} : V3{0.f, 0.f, 0.f};
@@ -817,7 +998,8 @@ __device__ __forceinline__ void group_pose_rows(const Group<G>& g, const Tabs& t
             }
         }
     }
-    for (int r = g.lane; r < 3 * ne; r += G) w.Jc()[r * Dp + D] = w.rpose()[3 * e0 + r];
+    const int nrows = (e1 < t.h->npose ? t.pose()[e1].r0 : t.h->pose_rows) - rbase;
+    for (int r = g.lane; r < nrows; r += G) w.Jc()[r * Dp + D] = w.rpose()[rbase + r];
     g.sync();
 }
 
@@ -857,7 +1039,7 @@ __device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Ta
     g.sync();
 }
 
-template <int G>
+template <int G, bool F = true>
 __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t, Ws& w, const EvalOut& ev, const float* base) {
     const TabHeader* h = t.h;
     const int D = h->D, T = h->T, E = h->E;
@@ -879,12 +1061,13 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
         w.Hc()[e] = 0.f;
     }
     g.sync();
-    // pose rows, kChunkRows/3 entries per chunk
-    constexpr int PE = kChunkRows / 3;
-    for (int e0 = 0; e0 < h->npose; e0 += PE) {
-        const int ne = min(PE, h->npose - e0);
-        group_pose_rows<G>(g, t, w, Tj, S, base, e0, ne);
-        group_accumulate_chunk<G>(g, t, w, 3 * ne);
+    // pose rows, as many whole entries per chunk as fit
+    group_frame_factors<G, F>(g, t, w, Tj, base);
+    for (int e0 = 0; e0 < h->npose;) {
+        const int e1 = pose_chunk_end(t, e0);
+        group_pose_rows<G, F>(g, t, w, Tj, S, base, e0, e1);
+        group_accumulate_chunk<G>(g, t, w, (e1 < h->npose ? t.pose()[e1].r0 : h->pose_rows) - t.pose()[e0].r0);
+        e0 = e1;
     }
     // collision rows
     for (int ci = 0; ci < h->ncoll; ++ci) {

@@ -184,7 +184,10 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
         float* Jo = Jout ? Jout + (size_t)p * R * D : nullptr;
         // residuals
         if (ro) {
-            for (int r = g.lane; r < 3 * h->npose; r += G) ro[t.pose()[r / 3].out_row + r % 3] = w.rpose()[r];
+            for (int e = g.lane; e < h->npose; e += G) {
+                const PoseEntry& pe = t.pose()[e];
+                for (int k = 0; k < pose_entry_rows(pe); ++k) ro[pe.out_row + k] = w.rpose()[pe.r0 + k];
+            }
             if (h->has_limit)
                 for (int a = g.lane; a < h->na; a += G) ro[h->limit_row + a] = w.rlim()[a];
         }
@@ -202,16 +205,21 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
         }
         g.sync();
         if (Jo) {
-            constexpr int PE = kChunkRows / 3;
-            for (int e0 = 0; e0 < h->npose; e0 += PE) {
-                const int ne = min(PE, h->npose - e0);
-                group_pose_rows<G>(g, t, w, ev.Tj, S, b, e0, ne);
-                for (int it = g.lane; it < 3 * ne * D; it += G) {
+            group_frame_factors<G>(g, t, w, ev.Tj, b);
+            for (int e0 = 0; e0 < h->npose;) {
+                const int e1 = pose_chunk_end(t, e0);
+                group_pose_rows<G>(g, t, w, ev.Tj, S, b, e0, e1);
+                const int rbase = t.pose()[e0].r0;
+                const int nr = (e1 < h->npose ? t.pose()[e1].r0 : h->pose_rows) - rbase;
+                for (int it = g.lane; it < nr * D; it += G) {
                     const int rr = it / D, c = it - rr * D;
-                    const int row = t.pose()[e0 + rr / 3].out_row + rr % 3;
+                    int el = e0;
+                    while (t.pose()[el].r0 + pose_entry_rows(t.pose()[el]) <= rbase + rr) ++el;
+                    const int row = t.pose()[el].out_row + (rbase + rr - t.pose()[el].r0);
                     Jo[(size_t)row * D + c] = w.Jc()[rr * Dp + c];
                 }
                 g.sync();
+                e0 = e1;
             }
             if (h->has_limit)
                 for (int a = g.lane; a < h->na; a += G) {

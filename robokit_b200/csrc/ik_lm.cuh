@@ -84,7 +84,7 @@ struct StepTrace {  // optional per-step outputs (ik_step)
 //         returns false (the caller applies its start rules).
 //  else:  one LM iteration from the cached linearisation (LMOptimizer._step_body,
 //         lm_optimizer.py:834-1005); returns true when the problem stops.
-template <int G>
+template <int G, bool F = true>
 __device__ __forceinline__ bool group_step(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
                                            bool fresh, StepTrace* trace = nullptr) {
     const bool floating = t.h->base_off != 0;
@@ -98,7 +98,7 @@ __device__ __forceinline__ bool group_step(const Group<G>& g, const Tabs& t, Ws&
         }
         group_integrate<G>(g, t, w, w.q, w.base, w.qp, w.basep);
     }
-    const EvalOut ev = group_eval<G>(g, t, w, fresh ? w.q : w.qp, floating ? (fresh ? w.base : w.basep) : nullptr);
+    const EvalOut ev = group_eval<G, F>(g, t, w, fresh ? w.q : w.qp, floating ? (fresh ? w.base : w.basep) : nullptr);
     bool acc = true;
     if (!fresh) {
         // gain ratio in FP64 (lm_optimizer.py:319-329)
@@ -133,7 +133,7 @@ __device__ __forceinline__ bool group_step(const Group<G>& g, const Tabs& t, Ws&
         st.cost = ev.cost;
         st.pos_err = ev.max_pos;
         st.rot_err = ev.max_rot;
-        group_linearize<G>(g, t, w, ev, floating ? w.base : nullptr);
+        group_linearize<G, F>(g, t, w, ev, floating ? w.base : nullptr);
     } else {
         st.lambda = fminf(fmaxf(st.lambda * P.lambda_factor, P.lambda_min), P.lambda_max);
     }
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_plain_kernel(const char* 
 // persistent form: groups pull problems from a device work queue and iterate
 // each to its own stop rule inside the launch.
 // ---------------------------------------------------------------------------
-template <int G>
+template <int G, bool F = true>
 __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const char* __restrict__ blob, int batch,
                                                                      float* q, float* base, IkLmParams P,
                                                                      int* queue, float* out_cost, float* out_lambda,
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(kBlockThreads, 4) lm_persistent_kernel(const c
             continue;
         }
         if (p >= 0) {
-            bool stop = group_step<G>(g, t, w, st, P, fresh);
+            bool stop = group_step<G, F>(g, t, w, st, P, fresh);
             if (fresh) stop = start_stops<G>(st, P);
             fresh = false;
             if (stop) {

@@ -30,20 +30,22 @@ IK_HD inline constexpr int ws_stride(int ws_bytes, int G) { return ((ws_bytes + 
 // pose-entry kinds
 constexpr int kPosePosition = 0;
 constexpr int kPoseRotation = 1;
+constexpr int kPoseFrame = 2;   // six rows: SE(3) log of T_frame^-1 T_target (frame_task.py:505-527)
 
 // One block of three residual rows: a PositionTask or RotationTask frame.
 struct PoseEntry {
     int32_t link;         // link index of the frame
-    int32_t kind;         // kPosePosition / kPoseRotation
+    int32_t kind;         // kPosePosition / kPoseRotation / kPoseFrame
     int32_t term;         // term index in the user's list
     int32_t frame;        // frame index inside the term
     int32_t num_frames;   // frames of the owning term (target row stride)
     int32_t out_row;      // first row in the reference layout
     int32_t target_rows;  // rows of the target array (broadcast rule)
-    int32_t pad0;
-    float w[4];           // row weights (3 used)
+    int32_t r0;           // first row of this entry among all pose rows
+    float w[4];           // row weights (3 used); a frame entry: w[0] translation, w[1] rotation rows
     const float* targets; // device pointer [target_rows, num_frames, 7]
-    int64_t pad1;
+    int32_t fm;           // frame entry: slot of its Jacobian factors in the workspace, else -1
+    int32_t pad1;
 };
 static_assert(sizeof(PoseEntry) == 64, "PoseEntry layout");
 
@@ -91,6 +93,9 @@ struct TabHeader {
     int32_t w_q, w_qp, w_base, w_basep, w_d32, w_misc;
     int32_t Dp;           // padded row stride of the Jacobian chunk
     int32_t max_slots;    // sum of slot-mode K over collision terms
+    int32_t pose_rows;    // rows of all pose entries (3 per position/rotation entry, 6 per frame entry)
+    int32_t nframe;       // frame entries
+    int32_t w_fM;         // workspace: 18 floats per frame entry (Jacobian factors P, K)
     // lane-per-problem workspace (float offsets; float k of lane t at [k * blockDim + t])
     int32_t thread_ok;    // 1 when the lane-per-problem kernels can run this problem
     int32_t t_floats;

@@ -27,7 +27,7 @@ from ...opt.lm_optimizer import LMOptimizer, LMOptimizerConfig
 from ...opt.sampler import RobertsSampler
 from ...opt.var_values import VarKey, VarValues
 from ...robo.robot_state import RobotState
-from ...terms.dense import PositionLimit, PositionTask, RotationTask, SelfCollisionTask, _PoseTask
+from ...terms.dense import FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask, _PoseTask
 from ...terms.task import Context
 from .config import IKContext, IKSolverConfig
 
@@ -81,7 +81,11 @@ class IKSolver:
                     [self.target_links[0]] if fi is IKContext.TARGET_LINK else fi)
                 if tg is not IKContext.TARGET and not isinstance(tg, Context):
                     raise NotImplementedError("IKSolver pose templates take T_world_target=IKContext.TARGET")
-                out.append(type(t)(self.robot, frames, targets, weight=t.weight))
+                if isinstance(t, FrameTask):
+                    out.append(FrameTask(self.robot, frames, targets, position_weight=t.position_weight,
+                                         orientation_weight=t.orientation_weight))
+                else:
+                    out.append(type(t)(self.robot, frames, targets, weight=t.weight))
             elif isinstance(t, PositionLimit):
                 out.append(PositionLimit(self.robot, weight=t.weight))
             elif isinstance(t, SelfCollisionTask):

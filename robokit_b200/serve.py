@@ -62,7 +62,7 @@ class IKServer:
         keep: List[Any] = []
         descs = lower_terms(robot, list(terms), 1, floating, keep)
         pose_frames = [int(descs[i].num_frames) for i in range(len(terms))
-                       if descs[i].kind in (N.IK_TERM_POSITION, N.IK_TERM_ROTATION)]
+                       if descs[i].kind in (N.IK_TERM_POSITION, N.IK_TERM_ROTATION, N.IK_TERM_FRAME)]
         mask = None
         if active_dof_mask is not None:
             mask = np.ascontiguousarray(active_dof_mask, np.float32)

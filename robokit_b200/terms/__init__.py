@@ -1,5 +1,5 @@
-from .dense import PositionLimit, PositionTask, RotationTask, SelfCollisionTask
+from .dense import FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask
 from .task import Context, NativeProblem, ResidualTask, Task
 
-__all__ = ["Context", "NativeProblem", "PositionLimit", "PositionTask", "ResidualTask", "RotationTask",
+__all__ = ["Context", "FrameTask", "NativeProblem", "PositionLimit", "PositionTask", "ResidualTask", "RotationTask",
            "SelfCollisionTask", "Task"]

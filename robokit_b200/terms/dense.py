@@ -157,6 +157,45 @@ class RotationTask(_PoseTask):
         super().__init__(robot, frame_index, T_world_target, weight, fixed_target, name)
 
 
+class FrameTask(_PoseTask):
+    """w (.) log(T_frame^-1 T_target), six rows per frame; Jacobian -w (.) jlog Ad(T_frame^-1) S
+    (frame_task.py:47-621, residual_mode "log")."""
+
+    kind = N.IK_TERM_FRAME
+
+    def __init__(self, robot: Any = None, frame_index: Any = None, T_world_target: Any = None,
+                 position_weight: Union[float, Sequence[float]] = 1.0,
+                 orientation_weight: Union[float, Sequence[float]] = 1.0,
+                 residual_mode: Literal["log", "distance"] = "log", trajectory_frames: int = 1, name: str = ""):
+        if residual_mode not in {"log", "distance"}:
+            raise ValueError(f"Unsupported residual_mode: {residual_mode}")
+        if residual_mode != "log":
+            raise NotImplementedError("residual_mode='distance' is outside the IK hot path (log residuals only)")
+        if trajectory_frames != 1:
+            raise NotImplementedError("trajectory frames are outside the IK hot path")
+        self.position_weight = position_weight
+        self.orientation_weight = orientation_weight
+        self.residual_mode = residual_mode
+        super().__init__(robot, frame_index, T_world_target, 1.0, False, name)
+
+    def _set_weight_array(self, weight: Any) -> None:
+        pw = np.broadcast_to(np.asarray(self.position_weight, np.float32), (self.num_frames,))
+        ow = np.broadcast_to(np.asarray(self.orientation_weight, np.float32), (self.num_frames,))
+        self.residual_weight = np.ascontiguousarray(np.stack([pw, ow], axis=1).reshape(-1))
+
+    def set_weight(self, position_weight: Any = None, orientation_weight: Any = None) -> None:
+        if position_weight is not None:
+            self.position_weight = position_weight
+        if orientation_weight is not None:
+            self.orientation_weight = orientation_weight
+        self._set_weight_array(None)
+        self._touch()
+
+    @property
+    def residual_dim(self) -> int:
+        return 6 * self.num_frames
+
+
 class PositionLimit(ResidualTask):
     """Joint-limit hinge w (max(0, q - hi) + max(0, lo - q)) (position_limit.py:185-573, mode "abs")."""
 

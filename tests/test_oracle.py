@@ -188,3 +188,40 @@ def test_oracle_lm_reaches_reachable_targets():
     # multithreaded and single-threaded solves agree exactly
     out1 = oracle.solve(rob, terms, prm, cfg.workload.q0, threads=1)
     np.testing.assert_array_equal(out1["q"], out["q"])
+
+
+def test_oracle_frame_term_matches_finite_differences(panda_spec):
+    """FrameTask ("log") residual and Jacobian of the oracle vs central differences (joint columns),
+    with and without a floating base; the residual is zero at the frame's own pose."""
+    spec = panda_spec
+    rob = oracle.Robot.from_spec(spec)
+    hand = spec.link_names.index("panda_hand")
+    link4 = spec.link_names.index("panda_link4")
+    rng = np.random.default_rng(3)
+    q = (spec.midrange_q + rng.normal(0, 0.3, spec.num_actuated_joints)).astype(np.float64)
+    tgt = np.array([[[0.3, -0.2, 0.6, 0.7, 0.2, -0.5, 0.4], [0.1, 0.3, 0.4, 0.2, 0.9, 0.1, -0.3]]], np.float32)
+    tgt[..., 3:] /= np.linalg.norm(tgt[..., 3:], axis=-1, keepdims=True)
+    terms = oracle.Terms([dict(kind=5, num_frames=2, frame_links=[hand, link4], weights=[2.0, 0.7, 1.0, 3.0],
+                               targets=tgt, target_rows=1)])
+    for base in (None, np.array([[0.1, -0.2, 0.3, 0.9, 0.1, -0.3, 0.2]])):
+        if base is not None:
+            base[:, 3:] /= np.linalg.norm(base[:, 3:])
+            base = base.astype(np.float32)
+        boff = 0 if base is None else 6
+        r, J = oracle.residual_jacobian(rob, terms, q[None].astype(np.float32), base)
+        assert r.shape == (1, 12)
+        eps = 1e-3
+        for a in range(spec.num_actuated_joints):
+            qp, qm = q.copy(), q.copy()
+            qp[a] += eps
+            qm[a] -= eps
+            rp, _ = oracle.residual_jacobian(rob, terms, qp[None].astype(np.float32), base)
+            rm, _ = oracle.residual_jacobian(rob, terms, qm[None].astype(np.float32), base)
+            np.testing.assert_allclose(J[0][:, boff + a], (rp[0] - rm[0]) / (2 * eps), atol=5e-3)
+    # at the frame's own pose the residual vanishes
+    T_link = oracle.fk(rob, q[None].astype(np.float32))["T_link"]
+    own = np.stack([T_link[0, hand], T_link[0, link4]])[None].astype(np.float32)
+    r0, _ = oracle.residual_jacobian(rob, oracle.Terms([dict(kind=5, num_frames=2, frame_links=[hand, link4],
+                                                             weights=[1.0] * 4, targets=own, target_rows=1)]),
+                                     q[None].astype(np.float32))
+    assert np.abs(r0).max() < 1e-6
