@@ -60,6 +60,9 @@ extern "C" {
 #define IK_TERM_SELF_COLLISION 4 /* terms/dense/self_collision_task.py:593     */
 #define IK_TERM_FRAME 5          /* terms/dense/frame_task.py:47 ("log" mode): six rows per frame,
                                     weights [num_frames*2] = (position, orientation) per frame */
+#define IK_TERM_JOINT_REF 6      /* w_a (q_a - ref_a), one row per actuated joint: SmoothnessTask
+                                    (smoothness_task.py:22) / ConfigurationTask (configuration_task.py:25),
+                                    joints only; weights [na]; d_targets = references [target_rows, na] */
 
 /* self-collision pair modes */
 #define IK_PAIRS_SLOTS 0 /* reference: <= K link pairs, most penetrating sphere pair each */
@@ -320,6 +323,13 @@ int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, cons
 int ik_select_best(int32_t batch, int32_t num_candidates, int32_t keep, const float* d_cost, const float* d_q,
                    const float* d_base, int32_t num_actuated, float* d_q_out, float* d_base_out, float* d_cost_out,
                    int32_t* d_index_out, void* stream);
+
+/* Keep the previous solution where it scores no worse, IKSolver.solve
+ * (helpers/ik/ik.py:43-56, 259-289): rows with d_prev_cost[b] <= d_cost[b] copy
+ * d_prev_q (num_actuated per row) and, when both are given, d_prev_base (7 per
+ * row) over d_q / d_base.  Costs are left as they are. */
+int ik_keep_previous(int32_t batch, int32_t num_actuated, const float* d_prev_cost, const float* d_cost,
+                     const float* d_prev_q, const float* d_prev_base, float* d_q, float* d_base, void* stream);
 
 /* Clamp joints to [lo, hi], RobotState.clamp_q (robo/robot_state.py:314-333,
  * robot_kernels.py:593-609); entries whose d_mask is 0 are left (mask may be NULL). */

@@ -429,7 +429,7 @@ int or_residual_dim(const OrRobot* r, const OrTerm* terms, int32_t nterms) {
             R += 3 * t->num_frames;
         else if (t->kind == 5)
             R += 6 * t->num_frames;
-        else if (t->kind == 3)
+        else if (t->kind == 3 || t->kind == 6)
             R += r->na;
         else if (t->kind == 4)
             R += t->pair_mode == 0 ? t->max_active_pairs : t->num_sphere_pairs;
@@ -558,6 +558,23 @@ static void eval_terms(const OrRobot* r, const OrTerm* terms, int nterms, int fl
                     for (int c = 0; c < D; ++c) J[(size_t)(row + a) * D + c] = 0.0;
                     const double sg = v > hi ? 1.0 : (v < lo ? -1.0 : 0.0);
                     J[(size_t)(row + a) * D + boff + a] = t->weights[a] * sg;
+                }
+            }
+            row += r->na;
+        } else if (t->kind == 6) {
+            /* smoothness_task.py:350-366, configuration_task.py:322-334:
+             * r_a = w_a (q_a - ref_a), the reference row repeated over batch / rows problems */
+            const int rows = t->target_rows > 0 ? t->target_rows : B;
+            int rep = B / rows;
+            if (rep < 1) rep = 1;
+            int rr = b / rep;
+            if (rr > rows - 1) rr = rows - 1;
+            const float* ref = t->targets + (size_t)rr * r->na;
+            for (int a = 0; a < r->na; ++a) {
+                res[row + a] = t->weights[a] * (q[a] - (double)ref[a]);
+                if (J) {
+                    for (int c = 0; c < D; ++c) J[(size_t)(row + a) * D + c] = 0.0;
+                    J[(size_t)(row + a) * D + boff + a] = t->weights[a];
                 }
             }
             row += r->na;

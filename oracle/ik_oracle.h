@@ -35,11 +35,12 @@ typedef struct OrRobot {
 } OrRobot;
 
 typedef struct OrTerm {
-    int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision, 5 frame ("log") */
+    int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision, 5 frame ("log"),
+                     6 joint reference (smoothness / configuration, joints only) */
     int32_t num_frames;
     const int32_t* frame_links;
     const float* weights;
-    const float* targets; /* host [target_rows, num_frames, 7] */
+    const float* targets; /* host [target_rows, num_frames, 7]; kind 6: [target_rows, na] */
     int32_t target_rows;
     float margin;
     int32_t max_active_pairs;

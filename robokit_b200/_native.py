@@ -36,6 +36,7 @@ IK_TERM_ROTATION = 2
 IK_TERM_POSITION_LIMIT = 3
 IK_TERM_SELF_COLLISION = 4
 IK_TERM_FRAME = 5
+IK_TERM_JOINT_REF = 6
 
 IK_PAIRS_SLOTS = 0
 IK_PAIRS_ALL = 1
@@ -193,6 +194,7 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp],
     ),
+    "ik_keep_previous": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ik_clamp_q": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp]),
     "ik_malloc": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_size_t]),
     "ik_free": (ctypes.c_int, [_vp]),

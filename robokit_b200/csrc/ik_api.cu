@@ -130,6 +130,7 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_tgt = take(npose * 8 * 4);
     h->w_rpose = take(std::max(h->pose_rows, 3 * npose) * 4);
     h->w_fM = take(h->nframe * 18 * 4);
+    h->w_jref = take(h->njref * na * 4);
     h->w_rlim = take(na * 4);
     // The Jacobian chunk and its row records live only inside a linearisation and
     // the FP64 factor only inside a solve: they share one region.
@@ -233,8 +234,9 @@ int check_launch() {
     return IK_OK;
 }
 
+// The persistent kernel without the frame and joint-reference paths.
 template <int G>
-constexpr auto lm_persistent_noframe = lm_persistent_kernel<G, false>;
+constexpr auto lm_persistent_core = lm_persistent_kernel<G, false>;
 
 // Dispatch a templated kernel on the group width.
 #define IK_DISPATCH(G, KERNEL, ...)                                   \
@@ -574,10 +576,25 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
             for (int a = 0; a < r.na; ++a) limw[a] = th.weights[a];
         }
     }
+    // joint-reference terms: weights into the blob, entries after
+    std::vector<JointRefEntry> jref;
+    for (size_t ti = 0; ti < terms.size(); ++ti) {
+        const TermHost& th = terms[ti];
+        if (th.d.kind != IK_TERM_JOINT_REF) continue;
+        JointRefEntry e;
+        std::memset(&e, 0, sizeof(e));
+        e.out_row = th.row;
+        e.target_rows = th.d.target_rows;
+        e.o_w = b.addv(th.weights);
+        e.ws_ref = 0;  // set with the workspace layout
+        e.ref = th.d.d_targets;
+        jref.push_back(e);
+    }
     h = b.hdr();
     h->npose = (int)pose.size();
     h->pose_rows = pose_rows;
     h->nframe = nframe;
+    h->njref = (int)jref.size();
     h->has_limit = has_limit;
     h->limit_row = limit_row;
     // collision arrays
@@ -613,6 +630,8 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     b.hdr()->o_pose = o;
     const int o_coll = b.add(coll.data(), coll.size() * sizeof(CollEntry));
     b.hdr()->o_coll = o_coll;
+    const int o_jref = b.add(jref.data(), jref.size() * sizeof(JointRefEntry));
+    b.hdr()->o_jref = o_jref;
     o = b.addv(limw);
     b.hdr()->o_limw = o;
     std::vector<float> mask = mask_in;
@@ -628,6 +647,8 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0, h->ncoll > 0);
     CollEntry* ce = reinterpret_cast<CollEntry*>(b.buf.data() + o_coll);
     for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
+    JointRefEntry* je = reinterpret_cast<JointRefEntry*>(b.buf.data() + o_jref);
+    for (size_t i = 0; i < jref.size(); ++i) je[i].ws_ref = h->w_jref / 4 + (int)i * h->na;
     // lane-per-problem layout: small systems with all-pairs collision terms only
     {
         int off = 0;
@@ -646,7 +667,7 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         h->t_qp = take(std::max(h->na, 1));
         h->t_base = take(h->base_off ? 7 : 0);
         h->t_basep = take(h->base_off ? 7 : 0);
-        bool ok = h->D <= kSmallD && h->nframe == 0;
+        bool ok = h->D <= kSmallD && h->nframe == 0 && h->njref == 0;
         for (size_t i = 0; i < coll.size(); ++i) {
             if (ce[i].mode != IK_PAIRS_ALL) ok = false;
             ce[i].t_mask = take((ce[i].nsp + 31) / 32);
@@ -690,6 +711,11 @@ int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc*
             const int per = d.kind == IK_TERM_FRAME ? 2 : 3;
             th.weights.assign(d.weights, d.weights + per * d.num_frames);
             th.rows = (d.kind == IK_TERM_FRAME ? 6 : 3) * d.num_frames;
+        } else if (d.kind == IK_TERM_JOINT_REF) {
+            if (!d.weights && r.na > 0) return fail(IK_E_INVALID, "term %d: joint weights are NULL", i);
+            if (!d.d_targets) return fail(IK_E_INVALID, "term %d: joint-reference term needs a reference array", i);
+            th.weights.assign(d.weights, d.weights + r.na);
+            th.rows = r.na;
         } else if (d.kind == IK_TERM_POSITION_LIMIT) {
             if (++nlimit > 1) {
                 return fail(IK_E_UNSUPPORTED, "more than one PositionLimit term");
@@ -891,7 +917,8 @@ int ik_problem_set_targets(IkProblem* P, int32_t term_index, const float* d_targ
     if (!P) return fail(IK_E_INVALID, "problem is NULL");
     if (term_index < 0 || term_index >= (int)P->terms.size()) return fail(IK_E_INVALID, "term %d out of range", term_index);
     TermHost& th = P->terms[term_index];
-    if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION && th.d.kind != IK_TERM_FRAME)
+    if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION && th.d.kind != IK_TERM_FRAME &&
+        th.d.kind != IK_TERM_JOINT_REF)
         return fail(IK_E_INVALID, "term %d has no pose targets", term_index);
     if (!d_targets) return fail(IK_E_INVALID, "targets are NULL");
     th.d.d_targets = d_targets;
@@ -995,9 +1022,10 @@ int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, 
     }
     const int G = problem_group(P);
     const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
-    if (reinterpret_cast<const TabHeader*>(P->blob.data())->nframe == 0) {
-        // no frame entries: the kernel without the frame paths (a smaller instruction footprint)
-        IK_DISPATCH(G, lm_persistent_noframe, {
+    const TabHeader* th = reinterpret_cast<const TabHeader*>(P->blob.data());
+    if (th->nframe == 0 && th->njref == 0) {
+        // no frame or joint-reference entries: the kernel without those paths (a smaller instruction footprint)
+        IK_DISPATCH(G, lm_persistent_core, {
             rc = prepare_kernel(kfn, smem);
             if (rc) return rc;
             int grid = 0;
@@ -1314,6 +1342,18 @@ int ik_select_best(int32_t batch, int32_t num_candidates, int32_t keep, const fl
     const int blocks = (int)(((size_t)batch * 32 + threads - 1) / threads);
     select_best_kernel<<<blocks, threads, 0, S(stream)>>>(batch, num_candidates, keep, d_cost, d_q, d_base, num_actuated,
                                                         d_q_out, d_base_out, d_cost_out, d_index_out);
+    return check_launch();
+}
+
+int ik_keep_previous(int32_t batch, int32_t num_actuated, const float* d_prev_cost, const float* d_cost,
+                     const float* d_prev_q, const float* d_prev_base, float* d_q, float* d_base, void* stream) {
+    if (batch < 0 || num_actuated < 0) return fail(IK_E_INVALID, "negative size");
+    if (!d_prev_base != !d_base) return fail(IK_E_INVALID, "give both base arrays or neither");
+    const int w = num_actuated + (d_base ? 7 : 0);
+    if (batch == 0 || w == 0) return IK_OK;
+    if (!d_prev_cost || !d_cost || (num_actuated > 0 && (!d_prev_q || !d_q))) return fail(IK_E_INVALID, "NULL array");
+    keep_previous_kernel<<<elementwise_grid((long long)batch * w), 256, 0, S(stream)>>>(
+        batch, num_actuated, d_prev_cost, d_cost, d_prev_q, d_base ? d_prev_base : nullptr, d_q, d_base);
     return check_launch();
 }
 

@@ -364,6 +364,7 @@ struct Tabs {
     IK_TAB(int, jorder, o_jorder)
     IK_TAB(PoseEntry, pose, o_pose)
     IK_TAB(CollEntry, coll, o_coll)
+    IK_TAB(JointRefEntry, jref, o_jref)
     IK_TAB(float, limw, o_limw)
     IK_TAB(float, mask, o_mask)
     IK_TAB(uint16_t, ab, o_ab)
@@ -732,6 +733,16 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
             const float err = fmaxf(0.f, v - hi) + fmaxf(0.f, lo - v);
             const float r = t.limw()[a] * err;
             w.rlim()[a] = r;
+            kadd(ks, kc, r * r);
+        }
+    }
+    // joint references, smoothness_task.py:350-366 / configuration_task.py:322-334 (joints)
+    for (int je = 0; F && je < h->njref; ++je) {
+        const JointRefEntry& jr = t.jref()[je];
+        const float* wj = t.at<float>(jr.o_w);
+        const float* ref = reinterpret_cast<const float*>(w.raw) + jr.ws_ref;
+        for (int a = g.lane; a < h->na; a += G) {
+            const float r = wj[a] * (q[a] - ref[a]);
             kadd(ks, kc, r * r);
         }
     }
@@ -1163,6 +1174,11 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
                 const float js = t.limw()[k] * sg;
                 v += js * js;
             }
+            if (F && a == b && a >= boff)
+                for (int je = 0; je < h->njref; ++je) {
+                    const float wk = t.at<float>(t.jref()[je].o_w)[a - boff];
+                    v += wk * wk;
+                }
         } else {
             a = e - T;
             b = a;
@@ -1173,6 +1189,12 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
                 const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
                 v += t.limw()[k] * sg * w.rlim()[k];
             }
+            if (F && a >= boff)
+                for (int je = 0; je < h->njref; ++je) {
+                    const JointRefEntry& jr = t.jref()[je];
+                    const float wk = t.at<float>(jr.o_w)[a - boff];
+                    v += wk * (wk * (w.q[a - boff] - reinterpret_cast<const float*>(w.raw)[jr.ws_ref + a - boff]));
+                }
         }
         if (h->mask_any) v *= (e < T) ? t.mask()[a] * t.mask()[b] : t.mask()[a];
         w.Hs()[e] = v;

@@ -190,6 +190,12 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
             }
             if (h->has_limit)
                 for (int a = g.lane; a < h->na; a += G) ro[h->limit_row + a] = w.rlim()[a];
+            for (int je = 0; je < h->njref; ++je) {
+                const JointRefEntry& jr = t.jref()[je];
+                const float* wj = t.at<float>(jr.o_w);
+                const float* ref = reinterpret_cast<const float*>(w.raw) + jr.ws_ref;
+                for (int a = g.lane; a < h->na; a += G) ro[jr.out_row + a] = wj[a] * (w.q[a] - ref[a]);
+            }
         }
         float* S = ev.S;
         for (int j = g.lane; j < h->nj; j += G) {
@@ -228,6 +234,10 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                     const float sg = qv > hi ? 1.f : (qv < lo ? -1.f : 0.f);
                     Jo[(size_t)(h->limit_row + a) * D + boff + a] = t.limw()[a] * sg;
                 }
+            for (int je = 0; je < h->njref; ++je) {
+                const JointRefEntry& jr = t.jref()[je];
+                for (int a = g.lane; a < h->na; a += G) Jo[(size_t)(jr.out_row + a) * D + boff + a] = t.at<float>(jr.o_w)[a];
+            }
         }
         for (int ci = 0; ci < h->ncoll; ++ci) {
             const CollEntry& ce = t.coll()[ci];
@@ -504,6 +514,21 @@ __global__ void masked_copy_rows_kernel(int rows, int width, const int* mask, co
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const long long r = i / width;
         if (mask[r] == 1) dst[i] = src[i];
+    }
+}
+
+__global__ void keep_previous_kernel(int batch, int na, const float* prev_cost, const float* cost, const float* prev_q,
+                                     const float* prev_base, float* q, float* base) {
+    const int w = na + (base ? 7 : 0);
+    const long long n = (long long)batch * w;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long b = i / w;
+        const int c = (int)(i - b * w);
+        if (!(prev_cost[b] <= cost[b])) continue;
+        if (c < na)
+            q[b * na + c] = prev_q[b * na + c];
+        else
+            base[b * 7 + (c - na)] = prev_base[b * 7 + (c - na)];
     }
 }
 

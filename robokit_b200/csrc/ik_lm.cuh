@@ -45,6 +45,15 @@ __device__ __forceinline__ void load_point(const Group<G>& g, const Tabs& t, Ws&
 template <int G>
 __device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
     const TabHeader* h = t.h;
+    for (int je = 0; je < h->njref; ++je) {
+        const JointRefEntry& jr = t.jref()[je];
+        const int rows = jr.target_rows > 0 ? jr.target_rows : batch;
+        int rep = batch / rows;
+        if (rep < 1) rep = 1;
+        const int row = min(p / rep, rows - 1);
+        float* dst = reinterpret_cast<float*>(w.raw) + jr.ws_ref;
+        for (int a = g.lane; a < h->na; a += G) dst[a] = jr.ref[(size_t)row * h->na + a];
+    }
     const int items = h->npose * 7;
     for (int it = g.lane; it < items; it += G) {
         const int e = it / 7, c = it - 7 * e;
@@ -84,6 +93,8 @@ struct StepTrace {  // optional per-step outputs (ik_step)
 //         returns false (the caller applies its start rules).
 //  else:  one LM iteration from the cached linearisation (LMOptimizer._step_body,
 //         lm_optimizer.py:834-1005); returns true when the problem stops.
+// F = false compiles out the frame and joint-reference paths (for problems with
+// neither).
 template <int G, bool F = true>
 __device__ __forceinline__ bool group_step(const Group<G>& g, const Tabs& t, Ws& w, LmState& st, const IkLmParams& P,
                                            bool fresh, StepTrace* trace = nullptr) {

@@ -68,6 +68,19 @@ struct CollEntry {
 };
 static_assert(sizeof(CollEntry) == 64, "CollEntry layout");
 
+// One joint-reference term: rows w_a (q_a - ref_a) (SmoothnessTask with the
+// previous state, smoothness_task.py:350-366; ConfigurationTask toward a rest
+// configuration, configuration_task.py:25-120; joints only).
+struct JointRefEntry {
+    int32_t out_row;      // first row in the reference layout
+    int32_t target_rows;  // rows of the reference array (broadcast rule as for pose targets)
+    int32_t o_w;          // blob offset of the weights [na]
+    int32_t ws_ref;       // workspace float offset of this problem's reference [na]
+    const float* ref;     // device pointer [target_rows, na]
+    int64_t pad;
+};
+static_assert(sizeof(JointRefEntry) == 32, "JointRefEntry layout");
+
 struct TabHeader {
     int32_t bytes;        // blob size, multiple of 16
     int32_t nj, nl, na, ns;
@@ -96,6 +109,9 @@ struct TabHeader {
     int32_t pose_rows;    // rows of all pose entries (3 per position/rotation entry, 6 per frame entry)
     int32_t nframe;       // frame entries
     int32_t w_fM;         // workspace: 18 floats per frame entry (Jacobian factors P, K)
+    int32_t njref;        // joint-reference terms
+    int32_t o_jref;       // blob offset of the JointRefEntry table
+    int32_t w_jref;       // workspace: the references [njref * na]
     // lane-per-problem workspace (float offsets; float k of lane t at [k * blockDim + t])
     int32_t thread_ok;    // 1 when the lane-per-problem kernels can run this problem
     int32_t t_floats;

@@ -15,8 +15,15 @@ class IKContext(Context):
     """Values an IKSolver gives its term templates (helpers/ik/config.py:12-32)."""
 
     TARGET_LINKS = 0
+    """Indices of the target links."""
     TARGET_LINK = 1
+    """The first target link."""
     TARGET = 2
+    """Target poses (batch, links, 7), which candidates share."""
+    PREVIOUS_STATE = 3
+    """The previous solution (batch,), from solve(prev_state=...); zeros until the first one."""
+    REST_Q = 4
+    """Rest configurations (batch, dofs): the zero configuration until solve(rest_state=...)."""
 
 
 def _default_solver() -> PopulationSolverConfig:

@@ -9,9 +9,12 @@ target's best candidates by cost — and returns the final stage's candidates.
 Everything between the host call and the result runs on the GPU: the spread
 (integrate + clamp kernels), one persistent solve launch per stage and one
 select launch between stages.  The term templates of the config (PositionTask,
-RotationTask with IKContext placeholders, PositionLimit) become concrete terms
-that read the targets with the reference's broadcast rule (candidate c of
-target b reads target row b).
+RotationTask, FrameTask with IKContext placeholders, PositionLimit,
+SelfCollisionTask, SmoothnessTask on IKContext.PREVIOUS_STATE, ConfigurationTask
+on IKContext.REST_Q) become concrete terms that read the solver's target,
+previous-state and rest buffers in place with the reference's broadcast rule
+(candidate c of target b reads row b).  With a previous state, each target keeps
+it where it scores no worse than the solve's result (helpers/ik/ik.py:257-289).
 """
 
 from __future__ import annotations
@@ -27,7 +30,8 @@ from ...opt.lm_optimizer import LMOptimizer, LMOptimizerConfig
 from ...opt.sampler import RobertsSampler
 from ...opt.var_values import VarKey, VarValues
 from ...robo.robot_state import RobotState
-from ...terms.dense import FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask, _PoseTask
+from ...terms.dense import (ConfigurationTask, FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask,
+                            SmoothnessTask, _PoseTask)
 from ...terms.task import Context
 from .config import IKContext, IKSolverConfig
 
@@ -92,6 +96,23 @@ class IKSolver:
                 c = SelfCollisionTask(self.robot, t.weight, t.margin, max_active_pairs=t.max_active_pairs,
                                       filter_adjacent_links=t.filter_adjacent_links, pair_mode=t.pair_mode)
                 out.append(c)
+            elif isinstance(t, (SmoothnessTask, ConfigurationTask)) and t.robot is not None:
+                out.append(t)  # built with a robot: passes as is
+            elif isinstance(t, SmoothnessTask):
+                s = SmoothnessTask(self.robot, weight=t.weight, name=t.name)
+                if t.prev_var is IKContext.PREVIOUS_STATE:
+                    s.bind_previous(self._prev_q)
+                elif t.prev_var is not None:
+                    raise NotImplementedError("IKSolver smoothness templates take prev_var=IKContext.PREVIOUS_STATE")
+                out.append(s)
+            elif isinstance(t, ConfigurationTask):
+                c = ConfigurationTask(self.robot, rest_q=None if t.rest_q_arg is IKContext.REST_Q else t.rest_q_arg,
+                                      weight=t.weight, name=t.name, mask=t.mask)
+                if t.rest_q_arg is IKContext.REST_Q:
+                    c.bind_rest(self._rest_q)
+                elif isinstance(t.rest_q_arg, Context):
+                    raise NotImplementedError("IKSolver configuration templates take rest_q=IKContext.REST_Q")
+                out.append(c)
             else:
                 raise NotImplementedError(f"{type(t).__name__} is outside the IK hot path")
         return out
@@ -100,6 +121,8 @@ class IKSolver:
         spec = self.robot.spec
         na = spec.num_actuated_joints
         self._targets = N.DeviceArray.zeros((B, self.num_targets, 7))
+        self._prev_q = N.DeviceArray.zeros((B, na))  # IKContext.PREVIOUS_STATE: zeros until a prev_state
+        self._rest_q = N.DeviceArray.from_numpy(np.tile(spec.zero_q.astype(np.float32), (B, 1)))  # IKContext.REST_Q
         self._terms = self._concrete_terms(self._targets)
         self._pose_terms = [t for t in self._terms if isinstance(t, _PoseTask)]
         for t in self._pose_terms:  # every stage's problem reads the one target buffer
@@ -127,7 +150,24 @@ class IKSolver:
         self._params = [None if opt is None else opt.config.native_params() for (_, _, _, opt) in self._stages]
         self._stream = N.Stream()
         self._graph: Optional[N.Graph] = None
+        self._scorer: Optional[LMOptimizer] = None  # prices a previous state (built on the first one)
         self._batch = B
+
+    def _score_previous(self, prev_state: RobotState, stream: int) -> None:
+        """Cost of prev_state under the solve's terms, its smoothness rows zero (helpers/ik/ik.py:257-270)."""
+        B, na = self._batch, self.num_joints
+        if self._scorer is None:
+            self._prev_save = self.robot.state(np.zeros((B, na), np.float32))
+            self._prev_cost = N.DeviceArray.zeros(B)
+            self._scorer = LMOptimizer(self._terms, LMOptimizerConfig(max_iter=0, form="persistent"))
+            self._scorer.reset(VarValues({VarKey.ROBOT: self._prev_save}))
+            self._score_params = self._scorer.config.native_params()
+        N.check(N.lib().ik_memcpy_dtod(self._prev_save.q.ptr, prev_state.q.ptr, self._prev_q.nbytes, stream))
+        sc = self._scorer
+        sc._slice(B)
+        N.check(N.lib().ik_solve_persistent(sc.problem.handle, B, self._prev_save.q.ptr, None,
+                                            ctypes.byref(self._score_params), self._prev_cost.ptr, sc.lm.ptr,
+                                            sc.iterations.ptr, sc.status.ptr, stream))
 
     def warmup(self, batch_size: int) -> None:
         """Build the buffers and run one solve on identity targets."""
@@ -184,12 +224,15 @@ class IKSolver:
         for _, _, state, _ in self._stages:
             state.invalidate()
 
-    def solve(self, T_world_target: Any, init_state: Optional[RobotState] = None,
+    def solve(self, T_world_target: Any, prev_state: Optional[RobotState] = None,
+              init_state: Optional[RobotState] = None, rest_state: Optional[RobotState] = None,
               out_state: Optional[RobotState] = None, init_sample_range: Optional[float] = None) -> RobotState:
         """Solutions for every target, instance-major: (batch * num_solutions, dofs) (helpers/ik/ik.py:223-304).
 
-        Under cuda_graph_mode "full" the device work of a solve from the midrange seed is captured into one
-        CUDA graph at the first solve and replayed after it; the call returns once the solutions are ready."""
+        prev_state (batch,) fills IKContext.PREVIOUS_STATE and is kept for a target where it costs no more
+        than the solve's result; rest_state fills IKContext.REST_Q.  Under cuda_graph_mode "full" the device
+        work of a solve from the midrange seed is captured into one CUDA graph at the first solve and replayed
+        after it; the call returns once the solutions are ready."""
         if isinstance(T_world_target, np.ndarray) or not hasattr(T_world_target, "ptr"):
             T = np.ascontiguousarray(T_world_target, np.float32)
             if T.ndim == 2:
@@ -208,12 +251,26 @@ class IKSolver:
             self._build(B)
         elif B != self._batch:
             raise ValueError(f"Batch size mismatch: expected {self._batch}, got {B}")
+        if prev_state is not None:
+            if self.num_solutions != 1:
+                raise ValueError("prev_state requires an IK final stage with num_candidates=1.")
+            if prev_state.batch_size != B:
+                raise ValueError(f"prev_state batch size mismatch: expected {B}, got {prev_state.batch_size}")
+            if prev_state.has_floating_base:
+                raise NotImplementedError("a floating base in IKSolver is outside this build (fixed base only)")
+        if rest_state is not None and rest_state.batch_size != B:
+            raise ValueError(f"rest_state batch size mismatch: expected {B}, got {rest_state.batch_size}")
         st = self._stream.handle
         nbytes = self._targets.nbytes
         if host:
             N.check(N.lib().ik_memcpy_htod(self._targets.ptr, T.ctypes.data, nbytes, st))
         else:
             N.check(N.lib().ik_memcpy_dtod(self._targets.ptr, T.ptr, nbytes, st))
+        if prev_state is not None:
+            N.check(N.lib().ik_memcpy_dtod(self._prev_q.ptr, prev_state.q.ptr, self._prev_q.nbytes, st))
+            self._score_previous(prev_state, st)
+        if rest_state is not None:
+            N.check(N.lib().ik_memcpy_dtod(self._rest_q.ptr, rest_state.q.ptr, self._rest_q.nbytes, st))
         if init_state is not None:
             self._seed_around(init_state, self.config.sampler.scale if init_sample_range is None else init_sample_range,
                               st)
@@ -226,8 +283,11 @@ class IKSolver:
                 self._graph.launch()
         else:
             self._device_body(st)
-        N.check(N.lib().ik_stream_synchronize(st))
         final = self._stages[-1][2]
+        if prev_state is not None:
+            N.check(N.lib().ik_keep_previous(B, self.num_joints, self._prev_cost.ptr, self._cost[-1].ptr,
+                                             self._prev_save.q.ptr, None, final.q.ptr, None, st))
+        N.check(N.lib().ik_stream_synchronize(st))
         if out_state is not None:
             out_state.q.assign(final.q)
             out_state.invalidate()

@@ -1,5 +1,6 @@
-from .dense import FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask
+from .dense import (ConfigurationTask, FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask,
+                    SmoothnessTask)
 from .task import Context, NativeProblem, ResidualTask, Task
 
-__all__ = ["Context", "FrameTask", "NativeProblem", "PositionLimit", "PositionTask", "ResidualTask", "RotationTask",
-           "SelfCollisionTask", "Task"]
+__all__ = ["ConfigurationTask", "Context", "FrameTask", "NativeProblem", "PositionLimit", "PositionTask", "ResidualTask",
+           "RotationTask", "SelfCollisionTask", "SmoothnessTask", "Task"]

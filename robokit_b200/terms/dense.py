@@ -1,8 +1,11 @@
 """Dense residual terms of the IK path.
 
 PositionTask (terms/dense/position_task.py:18-272), RotationTask
-(terms/dense/rotation_task.py:25-401), PositionLimit in "abs" mode
-(terms/dense/position_limit.py:185-573) and SelfCollisionTask with sphere
+(terms/dense/rotation_task.py:25-401), FrameTask in "log" mode
+(terms/dense/frame_task.py:47-621), PositionLimit in "abs" mode
+(terms/dense/position_limit.py:185-573), the joint blocks of SmoothnessTask
+(terms/dense/smoothness_task.py:22-460) and ConfigurationTask
+(terms/dense/configuration_task.py:25-478), and SelfCollisionTask with sphere
 geometry (terms/dense/self_collision_task.py:593-1152).  Constructor
 signatures, defaults, residual_dim and set_weight / set_target follow the
 reference; the arithmetic runs in libb200ik.so.
@@ -226,6 +229,210 @@ class PositionLimit(ResidualTask):
         w = np.zeros(na, np.float32)
         w[:] = 1.0 if self.weight is None else self.weight
         return dict(kind=N.IK_TERM_POSITION_LIMIT, weights=w)
+
+
+def _ref_rows(ref: Any, na: int) -> Any:
+    """A reference as [rows, na]: a DeviceArray (read in place) or a float32 numpy array."""
+    if isinstance(ref, N.DeviceArray) or hasattr(ref, "__cuda_array_interface__"):
+        d = N.as_device(ref, np.float32)
+        if d.size % max(na, 1) or d.size == 0:
+            raise ValueError(f"reference of shape {d.shape} does not hold rows of {na} joints")
+        return d.reshape((d.size // na, na))
+    a = np.ascontiguousarray(np.asarray(ref, np.float32).reshape(-1, na))
+    if a.shape[0] == 0:
+        raise ValueError("empty reference")
+    return a
+
+
+class _JointRefTask(ResidualTask):
+    """r_a = w_a (q_a - ref_a) over the actuated joints: a diagonal Jacobian block of w.
+
+    The reference row of problem b is b // max(1, batch // rows), the reference's
+    broadcast rule (smoothness_task.py:361-363, configuration_task.py:331-332)."""
+
+    _ref: Any = None
+    _ref_dev: Optional[N.DeviceArray] = None
+
+    def _joint_weights(self, na: int) -> np.ndarray:
+        w = np.zeros(na, np.float32)
+        w[:] = self.weight
+        return w
+
+    @property
+    def residual_dim(self) -> int:
+        return self.robot.spec.num_actuated_joints
+
+    def _reference(self, na: int) -> Any:
+        raise NotImplementedError
+
+    def _device_ref(self, na: int) -> N.DeviceArray:
+        ref = self._reference(na)
+        if isinstance(ref, N.DeviceArray):
+            return ref
+        if self._ref_dev is None or self._ref_dev.shape != ref.shape:
+            self._ref_dev = N.DeviceArray.from_numpy(ref)
+        else:
+            self._ref_dev.copy_from_numpy(ref)
+        return self._ref_dev
+
+    def _check(self, var: Any) -> int:
+        na = var.spec.num_actuated_joints
+        if self.robot is not None and self.robot.spec.num_actuated_joints != na:
+            raise ValueError("term built for another robot")
+        return na
+
+    def native_desc(self, var: Any) -> Dict[str, Any]:
+        na = self._check(var)
+        return dict(kind=N.IK_TERM_JOINT_REF, weights=self._joint_weights(na), targets=self._device_ref(na))
+
+    def host_desc(self, var: Any) -> Dict[str, Any]:
+        na = self._check(var)
+        ref = self._reference(na)
+        ref = ref.numpy() if isinstance(ref, N.DeviceArray) else ref
+        return dict(kind=N.IK_TERM_JOINT_REF, weights=self._joint_weights(na), targets=ref, target_rows=ref.shape[0])
+
+
+class SmoothnessTask(_JointRefTask):
+    """Penalise change from a previous joint state, w (q - q_prev) (smoothness_task.py:22-460).
+
+    Joints only: a floating-base previous state (whose base residual is an SE(3)
+    log) and the warm-up weight ramp are outside the IK hot path.  Without a
+    previous state the term adds zero rows, as the reference's does."""
+
+    def __init__(self, robot: Any = None, prev_var: Any = None, weight: Union[float, Sequence[float]] = 1.0,
+                 base_weight: Optional[Union[float, Sequence[float]]] = None, name: str = "", warmup_frames: int = 0,
+                 frame: Any = None):
+        if warmup_frames and frame is not None:
+            raise NotImplementedError("the warm-up weight ramp is outside the IK hot path")
+        if base_weight is not None or getattr(prev_var, "has_floating_base", False):
+            raise NotImplementedError("base smoothness residuals are outside the IK hot path (joints only)")
+        self.name = name
+        self.weight = weight
+        self.base_weight = base_weight
+        self.warmup_frames, self.frame = warmup_frames, frame
+        self.robot = robot
+        self.prev_var = prev_var
+        self._prev_q: Any = None
+        if prev_var is not None and not isinstance(prev_var, Context):
+            self._prev_q = _ref_rows(prev_var.q, prev_var.spec.num_actuated_joints)
+            if isinstance(self._prev_q, N.DeviceArray):  # the reference clones the state (smoothness_task.py:57)
+                self._prev_q = self._prev_q.clone()
+
+    @property
+    def active(self) -> bool:
+        return bool(np.any(self.weight))
+
+    def _joint_weights(self, na: int) -> np.ndarray:
+        w = super()._joint_weights(na)
+        return w if self._prev_q is not None else np.zeros_like(w)
+
+    def _reference(self, na: int) -> Any:
+        return self._prev_q if self._prev_q is not None else np.zeros((1, na), np.float32)
+
+    def set_weight(self, weight: Union[float, Sequence[float]]) -> None:
+        self.weight = weight
+        self._touch()
+
+    def bind_previous(self, prev_q: N.DeviceArray) -> None:
+        """Read the previous joints from `prev_q` [rows, na] in place from now on."""
+        self._prev_q = prev_q
+        self._touch()
+
+    def set_prev_state(self, prev_state: Any) -> None:
+        """Copy a new previous state in place; a new row count rebuilds (smoothness_task.py:111-120)."""
+        if getattr(prev_state, "has_floating_base", False):
+            raise NotImplementedError("base smoothness residuals are outside the IK hot path (joints only)")
+        new = _ref_rows(prev_state.q, prev_state.spec.num_actuated_joints)
+        if isinstance(self._prev_q, N.DeviceArray) and self._prev_q.shape == new.shape:
+            self._prev_q.assign(new)
+            return
+        self._prev_q = new.clone() if isinstance(new, N.DeviceArray) else new
+        self._touch()
+
+
+class ConfigurationTask(_JointRefTask):
+    """Bias joints toward a rest configuration, w (q - rest_q) (configuration_task.py:25-478).
+
+    ``rest_q`` is "midrange" (the joint-limit midpoints), an array of one or more
+    rows, or None (the zero configuration); ``mask`` scales each joint's weight.
+    The base rest pose (an SE(3) log residual) is outside the IK hot path."""
+
+    def __init__(self, robot: Any = None, rest_q: Any = None, T_world_base_rest: Any = None,
+                 weight: Union[float, Sequence[float]] = 1.0, base_weight: Any = None, include_joints: bool = True,
+                 var_key: Any = None, name: str = "", mask: Any = None):
+        if T_world_base_rest is not None or base_weight is not None:
+            raise NotImplementedError("base rest residuals are outside the IK hot path (joints only)")
+        if isinstance(rest_q, str) and rest_q != "midrange":
+            raise ValueError(f"Unsupported rest_q: {rest_q}")
+        if isinstance(mask, Context):
+            raise NotImplementedError("a helper's joint mask is outside the IK hot path")
+        self.name = name
+        self.weight = weight
+        self.base_weight = base_weight
+        self.include_joints = include_joints
+        self.mask = None if mask is None else np.asarray(mask, np.float32)
+        self.rest_q_arg = rest_q
+        self.robot = robot
+        self._rest: Any = None
+        if var_key is not None:
+            self.var_key = var_key
+
+    @property
+    def active(self) -> bool:
+        w = np.asarray(self.weight, np.float32)
+        if self.mask is not None and w.ndim <= 1:
+            w = w * self.mask
+        return bool(np.any(w))
+
+    def _joint_weights(self, na: int) -> np.ndarray:
+        w = super()._joint_weights(na)
+        if self.mask is not None:
+            w *= self.mask
+        return w
+
+    def _reference(self, na: int) -> Any:
+        if self._rest is not None:
+            return self._rest
+        r = self.rest_q_arg
+        if isinstance(r, Context):
+            raise ValueError("rest_q is a placeholder: build the term through a helper or give rest_q")
+        if isinstance(r, str):
+            spec = self.robot.spec if self.robot is not None else None
+            if spec is None:
+                raise ValueError('rest_q="midrange" needs a robot')
+            r = spec.midrange_q
+        elif r is None:
+            r = np.zeros(na, np.float32)
+        self._rest = _ref_rows(r, na)
+        return self._rest
+
+    def set_weight(self, weight: Union[float, Sequence[float]]) -> None:
+        self.weight = weight
+        self._touch()
+
+    def bind_rest(self, rest_q: N.DeviceArray) -> None:
+        """Read the rest joints from `rest_q` [rows, na] in place from now on."""
+        self._rest = rest_q
+        self._touch()
+
+    def set_target(self, rest_q: Any = None, T_world_base_rest: Any = None) -> None:
+        """Overwrite the rest joints in place; a new row count rebuilds (configuration_task.py:153-177)."""
+        if T_world_base_rest is not None:
+            raise NotImplementedError("base rest residuals are outside the IK hot path (joints only)")
+        if rest_q is None:
+            return
+        na = self.robot.spec.num_actuated_joints if self.robot is not None else np.asarray(rest_q).shape[-1]
+        new = _ref_rows(rest_q, na)
+        cur = self._rest
+        if cur is not None and cur.shape == new.shape:
+            if isinstance(cur, N.DeviceArray):
+                cur.assign(new)
+            else:
+                self._rest = new.numpy() if isinstance(new, N.DeviceArray) else new
+                self._touch()
+            return
+        self._rest = new
+        self._touch()
 
 
 class SelfCollisionTask(ResidualTask):

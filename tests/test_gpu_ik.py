@@ -64,16 +64,18 @@ def test_basic_preset_solves_panda_targets(gpu, panda_arm_spec):
 
 
 def test_single_stage_equals_the_optimizer(gpu, panda_arm_spec):
-    """One candidate, one stage: the solve is an LMOptimizer solve from the joint midrange (bitwise)."""
+    """One candidate, one stage: the solve is an LMOptimizer solve from the joint midrange (bitwise), its
+    smoothness term pulling toward the zero previous state the solver holds until a prev_state is given."""
     from robokit_b200.robo.robot import Robot
-    from robokit_b200.terms.dense import PositionLimit, PositionTask, RotationTask
+    from robokit_b200.terms.dense import PositionLimit, PositionTask, RotationTask, SmoothnessTask
 
     robot = Robot(panda_arm_spec)
     link = panda_arm_spec.link_names.index("panda_hand")
     T = _targets(robot, 64, 7, link)
     sol = IKSolver(presets.single_candidate, robot, link).solve(T).q.numpy()
     terms = [PositionTask(robot, [link], T, weight=20.0), RotationTask(robot, [link], T, weight=10.0),
-             PositionLimit(robot, weight=50.0)]
+             PositionLimit(robot, weight=50.0),
+             SmoothnessTask(robot, prev_var=robot.state(np.zeros((64, 7), np.float32)), weight=0.1)]
     opt = LMOptimizer(terms, LMOptimizerConfig(max_iter=30, lm_lambda=1.0, early_stopping_interval=0,
                                                form="persistent"))
     st = robot.state(np.tile(panda_arm_spec.midrange_q, (64, 1)).astype(np.float32))

@@ -85,3 +85,38 @@ def test_select_and_graph_argument_checks_need_no_device():
     assert lib.ik_graph_launch(None, None) == N.IK_E_INVALID
     assert lib.ik_graph_destroy(None) == N.IK_OK
     assert lib.ik_server_poll(None, None, 0, None) == N.IK_E_INVALID
+
+
+def test_joint_reference_terms_host_side(panda_spec):
+    """SmoothnessTask / ConfigurationTask lower to joint-reference rows; unsupported reference options raise."""
+    from robokit_b200.terms.dense import ConfigurationTask, SmoothnessTask
+
+    class _Robot:
+        spec = panda_spec
+
+    class _V:
+        spec, batch_size, has_floating_base = panda_spec, 4, False
+
+    na = panda_spec.num_actuated_joints
+    c = ConfigurationTask(_Robot(), rest_q="midrange", weight=0.5, mask=np.arange(na) % 2)
+    d = c.host_desc(_V)
+    assert d["kind"] == N.IK_TERM_JOINT_REF and d["target_rows"] == 1 and c.residual_dim == na
+    np.testing.assert_array_equal(d["targets"][0], panda_spec.midrange_q)
+    np.testing.assert_array_equal(d["weights"], 0.5 * (np.arange(na) % 2))
+    z = ConfigurationTask(_Robot(), weight=[1.0] * na).host_desc(_V)
+    assert not np.any(z["targets"])
+    s = SmoothnessTask(_Robot(), weight=0.1)
+    assert not np.any(s.host_desc(_V)["weights"])  # no previous state: zero rows
+    tmpl = SmoothnessTask(prev_var=IKContext.PREVIOUS_STATE, weight=0.1)
+    assert tmpl.active and tmpl.robot is None
+    with pytest.raises(NotImplementedError):
+        SmoothnessTask(_Robot(), base_weight=1.0)
+    with pytest.raises(NotImplementedError):
+        SmoothnessTask(_Robot(), warmup_frames=5, frame=IKContext.TARGET)
+    with pytest.raises(NotImplementedError):
+        ConfigurationTask(_Robot(), T_world_base_rest=np.zeros(7))
+    with pytest.raises(ValueError):
+        ConfigurationTask(_Robot(), rest_q="zero")
+    assert [type(t).__name__ for t in presets.smooth.terms] == ["PositionTask", "RotationTask", "PositionLimit",
+                                                                "SmoothnessTask"]
+    assert type(presets.single_candidate.terms[-1]).__name__ == "SmoothnessTask"

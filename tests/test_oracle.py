@@ -225,3 +225,26 @@ def test_oracle_frame_term_matches_finite_differences(panda_spec):
                                                              weights=[1.0] * 4, targets=own, target_rows=1)]),
                                      q[None].astype(np.float32))
     assert np.abs(r0).max() < 1e-6
+
+
+def test_oracle_joint_reference_term(panda_spec):
+    """Joint-reference rows (smoothness / rest): r = w (q - ref[b // (B // rows)]), J = diag(w) on the joint
+    columns, after the six base columns of a floating base."""
+    spec = panda_spec
+    rob = oracle.Robot.from_spec(spec)
+    na = spec.num_actuated_joints
+    rng = np.random.default_rng(7)
+    B = 6
+    q = rng.normal(0, 0.5, (B, na)).astype(np.float32)
+    ref = rng.normal(0, 0.5, (2, na)).astype(np.float32)  # 2 rows, 3 problems each
+    w = np.linspace(0.2, 1.5, na).astype(np.float32)
+    terms = oracle.Terms([dict(kind=6, weights=w, targets=ref, target_rows=2)])
+    assert oracle.residual_dim(rob, terms) == na
+    for base in (None, np.tile(np.array([[0.1, 0, 0, 1, 0, 0, 0]], np.float32), (B, 1))):
+        boff = 0 if base is None else 6
+        r, J = oracle.residual_jacobian(rob, terms, q, base)
+        rows = np.arange(B) // 3
+        np.testing.assert_allclose(r, w * (q.astype(np.float64) - ref[rows]), rtol=1e-12, atol=1e-12)
+        expect = np.zeros((B, na, boff + na))
+        expect[:, np.arange(na), boff + np.arange(na)] = w
+        np.testing.assert_array_equal(J, expect)
