@@ -63,6 +63,9 @@ extern "C" {
 #define IK_TERM_JOINT_REF 6      /* w_a (q_a - ref_a), one row per actuated joint: SmoothnessTask
                                     (smoothness_task.py:22) / ConfigurationTask (configuration_task.py:25),
                                     joints only; weights [na]; d_targets = references [target_rows, na] */
+#define IK_TERM_VELOCITY_LIMIT 7 /* w_a max(0, |q_a - prev_a| / dt - vmax_a), one row per actuated joint:
+                                    VelocityLimitTask (velocity_limit_task.py:14); weights [na];
+                                    d_targets = previous joints [target_rows, na]; dt, velocity_limits */
 
 /* self-collision pair modes */
 #define IK_PAIRS_SLOTS 0 /* reference: <= K link pairs, most penetrating sphere pair each */
@@ -124,6 +127,9 @@ typedef struct IkTermDesc {
     const int32_t* link_pair_offsets; /* [num_link_pairs+1] CSR into sphere_pairs        */
     int32_t num_sphere_pairs;
     const int32_t* sphere_pairs;      /* [num_sphere_pairs*2] grouped by link pair       */
+    /* velocity limit */
+    float dt;                         /* > 0                                              */
+    const float* velocity_limits;     /* host [na]                                        */
 } IkTermDesc;
 
 /* LMOptimizerConfig (opt/lm_optimizer.py:503-523) + OptimizerConfig

@@ -72,6 +72,8 @@ class OrTerm(ctypes.Structure):
         ("link_pair_offsets", ctypes.c_void_p),
         ("num_sphere_pairs", ctypes.c_int32),
         ("sphere_pairs", ctypes.c_void_p),
+        ("dt", ctypes.c_float),
+        ("velocity_limits", ctypes.c_void_p),
     ]
 
 
@@ -151,6 +153,8 @@ class Terms:
             arr[i].link_pair_offsets = keep(t.get("link_pair_offsets"), np.int32)
             arr[i].num_sphere_pairs = t.get("num_sphere_pairs", 0)
             arr[i].sphere_pairs = keep(t.get("sphere_pairs"), np.int32)
+            arr[i].dt = t.get("dt", 0.0)
+            arr[i].velocity_limits = keep(t.get("velocity_limits"), np.float32)
         self.arr = arr
         self.n = len(terms)
 

@@ -429,7 +429,7 @@ int or_residual_dim(const OrRobot* r, const OrTerm* terms, int32_t nterms) {
             R += 3 * t->num_frames;
         else if (t->kind == 5)
             R += 6 * t->num_frames;
-        else if (t->kind == 3 || t->kind == 6)
+        else if (t->kind == 3 || t->kind == 6 || t->kind == 7)
             R += r->na;
         else if (t->kind == 4)
             R += t->pair_mode == 0 ? t->max_active_pairs : t->num_sphere_pairs;
@@ -561,9 +561,12 @@ static void eval_terms(const OrRobot* r, const OrTerm* terms, int nterms, int fl
                 }
             }
             row += r->na;
-        } else if (t->kind == 6) {
-            /* smoothness_task.py:350-366, configuration_task.py:322-334:
-             * r_a = w_a (q_a - ref_a), the reference row repeated over batch / rows problems */
+        } else if (t->kind == 6 || t->kind == 7) {
+            /* kind 6 — smoothness_task.py:350-366, configuration_task.py:322-334:
+             *   r_a = w_a (q_a - ref_a);
+             * kind 7 — velocity_limit_task.py:188-232: qd = (q_a - prev_a) / dt,
+             *   r_a = w_a max(0, |qd| - vmax_a), J = w_a sign(qd) / dt where |qd| > vmax_a;
+             * the reference row repeated over batch / rows problems */
             const int rows = t->target_rows > 0 ? t->target_rows : B;
             int rep = B / rows;
             if (rep < 1) rep = 1;
@@ -571,10 +574,18 @@ static void eval_terms(const OrRobot* r, const OrTerm* terms, int nterms, int fl
             if (rr > rows - 1) rr = rows - 1;
             const float* ref = t->targets + (size_t)rr * r->na;
             for (int a = 0; a < r->na; ++a) {
-                res[row + a] = t->weights[a] * (q[a] - (double)ref[a]);
+                const double d = q[a] - (double)ref[a];
+                double rv = t->weights[a] * d, jv = t->weights[a];
+                if (t->kind == 7) {
+                    const double qd = d / (double)t->dt, vmax = t->velocity_limits[a];
+                    const int act = fabs(qd) > vmax;
+                    rv = act ? t->weights[a] * (fabs(qd) - vmax) : 0.0;
+                    jv = act ? t->weights[a] * (qd > 0 ? 1.0 : -1.0) / (double)t->dt : 0.0;
+                }
+                res[row + a] = rv;
                 if (J) {
                     for (int c = 0; c < D; ++c) J[(size_t)(row + a) * D + c] = 0.0;
-                    J[(size_t)(row + a) * D + boff + a] = t->weights[a];
+                    J[(size_t)(row + a) * D + boff + a] = jv;
                 }
             }
             row += r->na;

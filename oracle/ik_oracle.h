@@ -36,11 +36,12 @@ typedef struct OrRobot {
 
 typedef struct OrTerm {
     int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision, 5 frame ("log"),
-                     6 joint reference (smoothness / configuration, joints only) */
+                     6 joint reference (smoothness / configuration, joints only),
+                     7 velocity limit */
     int32_t num_frames;
     const int32_t* frame_links;
     const float* weights;
-    const float* targets; /* host [target_rows, num_frames, 7]; kind 6: [target_rows, na] */
+    const float* targets; /* host [target_rows, num_frames, 7]; kinds 6, 7: [target_rows, na] */
     int32_t target_rows;
     float margin;
     int32_t max_active_pairs;
@@ -50,6 +51,8 @@ typedef struct OrTerm {
     const int32_t* link_pair_offsets;
     int32_t num_sphere_pairs;
     const int32_t* sphere_pairs;
+    float dt;                     /* kind 7 */
+    const float* velocity_limits; /* kind 7: [na] */
 } OrTerm;
 
 typedef struct OrParams {

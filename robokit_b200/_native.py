@@ -37,6 +37,7 @@ IK_TERM_POSITION_LIMIT = 3
 IK_TERM_SELF_COLLISION = 4
 IK_TERM_FRAME = 5
 IK_TERM_JOINT_REF = 6
+IK_TERM_VELOCITY_LIMIT = 7
 
 IK_PAIRS_SLOTS = 0
 IK_PAIRS_ALL = 1
@@ -105,6 +106,8 @@ class IkTermDesc(ctypes.Structure):
         ("link_pair_offsets", _vp),
         ("num_sphere_pairs", ctypes.c_int32),
         ("sphere_pairs", _vp),
+        ("dt", ctypes.c_float),
+        ("velocity_limits", _vp),
     ]
 
 

@@ -580,7 +580,7 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     std::vector<JointRefEntry> jref;
     for (size_t ti = 0; ti < terms.size(); ++ti) {
         const TermHost& th = terms[ti];
-        if (th.d.kind != IK_TERM_JOINT_REF) continue;
+        if (th.d.kind != IK_TERM_JOINT_REF && th.d.kind != IK_TERM_VELOCITY_LIMIT) continue;
         JointRefEntry e;
         std::memset(&e, 0, sizeof(e));
         e.out_row = th.row;
@@ -588,6 +588,10 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         e.o_w = b.addv(th.weights);
         e.ws_ref = 0;  // set with the workspace layout
         e.ref = th.d.d_targets;
+        if (th.d.kind == IK_TERM_VELOCITY_LIMIT) {
+            e.o_vlim = b.addv(th.vlim);
+            e.dt = th.d.dt;
+        }
         jref.push_back(e);
     }
     h = b.hdr();
@@ -711,10 +715,16 @@ int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc*
             const int per = d.kind == IK_TERM_FRAME ? 2 : 3;
             th.weights.assign(d.weights, d.weights + per * d.num_frames);
             th.rows = (d.kind == IK_TERM_FRAME ? 6 : 3) * d.num_frames;
-        } else if (d.kind == IK_TERM_JOINT_REF) {
+        } else if (d.kind == IK_TERM_JOINT_REF || d.kind == IK_TERM_VELOCITY_LIMIT) {
             if (!d.weights && r.na > 0) return fail(IK_E_INVALID, "term %d: joint weights are NULL", i);
             if (!d.d_targets) return fail(IK_E_INVALID, "term %d: joint-reference term needs a reference array", i);
+            if (d.target_rows < 1) return fail(IK_E_INVALID, "term %d: target_rows %d", i, d.target_rows);
             th.weights.assign(d.weights, d.weights + r.na);
+            if (d.kind == IK_TERM_VELOCITY_LIMIT) {
+                if (!(d.dt > 0.f)) return fail(IK_E_INVALID, "dt must be positive");
+                if (!d.velocity_limits && r.na > 0) return fail(IK_E_INVALID, "term %d: velocity limits are NULL", i);
+                th.vlim.assign(d.velocity_limits, d.velocity_limits + r.na);
+            }
             th.rows = r.na;
         } else if (d.kind == IK_TERM_POSITION_LIMIT) {
             if (++nlimit > 1) {
@@ -918,7 +928,7 @@ int ik_problem_set_targets(IkProblem* P, int32_t term_index, const float* d_targ
     if (term_index < 0 || term_index >= (int)P->terms.size()) return fail(IK_E_INVALID, "term %d out of range", term_index);
     TermHost& th = P->terms[term_index];
     if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION && th.d.kind != IK_TERM_FRAME &&
-        th.d.kind != IK_TERM_JOINT_REF)
+        th.d.kind != IK_TERM_JOINT_REF && th.d.kind != IK_TERM_VELOCITY_LIMIT)
         return fail(IK_E_INVALID, "term %d has no pose targets", term_index);
     if (!d_targets) return fail(IK_E_INVALID, "targets are NULL");
     th.d.d_targets = d_targets;

@@ -658,6 +658,25 @@ __device__ __forceinline__ float pair_penetration(const Ws& w, int pk, float mar
 // lm_optimizer.py:964-982): FK, spheres, pose/limit/collision residuals,
 // cost = 0.5 |r|^2 and the pose errors of the metrics kernel (helpers/ik/ik.py:60-82).
 // ---------------------------------------------------------------------------
+// Row a of a joint-reference entry at joint value qa: residual r and the one
+// Jacobian entry js (column a).
+//  linear (o_vlim == 0): r = w (q - ref), js = w — smoothness_task.py:350-366,
+//    configuration_task.py:322-334;
+//  velocity hinge: qd = (q - prev) / dt, r = w max(0, |qd| - vmax),
+//    js = w sign(qd) / dt while |qd| > vmax, else 0 — velocity_limit_task.py:188-232.
+struct JrRow {
+    float r, js;
+};
+__device__ __forceinline__ JrRow jref_row(const Tabs& t, const Ws& w, const JointRefEntry& jr, float qa, int a) {
+    const float wa = t.at<float>(jr.o_w)[a];
+    const float d = qa - reinterpret_cast<const float*>(w.raw)[jr.ws_ref + a];
+    if (jr.o_vlim == 0) return JrRow{wa * d, wa};
+    const float qd = d / jr.dt;
+    const float vmax = t.at<float>(jr.o_vlim)[a];
+    if (fabsf(qd) > vmax) return JrRow{wa * (fabsf(qd) - vmax), wa * (qd > 0.f ? 1.f : -1.f) / jr.dt};
+    return JrRow{0.f, 0.f};
+}
+
 struct EvalOut {
     float cost;
     float max_pos;  // largest position error over position entries [m]
@@ -736,13 +755,11 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
             kadd(ks, kc, r * r);
         }
     }
-    // joint references, smoothness_task.py:350-366 / configuration_task.py:322-334 (joints)
+    // joint references (smoothness, rest) and velocity limits
     for (int je = 0; F && je < h->njref; ++je) {
         const JointRefEntry& jr = t.jref()[je];
-        const float* wj = t.at<float>(jr.o_w);
-        const float* ref = reinterpret_cast<const float*>(w.raw) + jr.ws_ref;
         for (int a = g.lane; a < h->na; a += G) {
-            const float r = wj[a] * (q[a] - ref[a]);
+            const float r = jref_row(t, w, jr, q[a], a).r;
             kadd(ks, kc, r * r);
         }
     }
@@ -1176,8 +1193,8 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
             }
             if (F && a == b && a >= boff)
                 for (int je = 0; je < h->njref; ++je) {
-                    const float wk = t.at<float>(t.jref()[je].o_w)[a - boff];
-                    v += wk * wk;
+                    const float js = jref_row(t, w, t.jref()[je], w.q[a - boff], a - boff).js;
+                    v += js * js;
                 }
         } else {
             a = e - T;
@@ -1191,9 +1208,8 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
             }
             if (F && a >= boff)
                 for (int je = 0; je < h->njref; ++je) {
-                    const JointRefEntry& jr = t.jref()[je];
-                    const float wk = t.at<float>(jr.o_w)[a - boff];
-                    v += wk * (wk * (w.q[a - boff] - reinterpret_cast<const float*>(w.raw)[jr.ws_ref + a - boff]));
+                    const JrRow row = jref_row(t, w, t.jref()[je], w.q[a - boff], a - boff);
+                    v += row.js * row.r;
                 }
         }
         if (h->mask_any) v *= (e < T) ? t.mask()[a] * t.mask()[b] : t.mask()[a];

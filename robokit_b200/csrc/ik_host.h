@@ -45,6 +45,7 @@ struct TermHost {
     IkTermDesc d;
     std::vector<int> frame_links;
     std::vector<float> weights;
+    std::vector<float> vlim;  // velocity-limit terms: [na]
     std::vector<int> lp, lpoff, sp;
     int row = 0, rows = 0;
 };

@@ -192,9 +192,7 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 for (int a = g.lane; a < h->na; a += G) ro[h->limit_row + a] = w.rlim()[a];
             for (int je = 0; je < h->njref; ++je) {
                 const JointRefEntry& jr = t.jref()[je];
-                const float* wj = t.at<float>(jr.o_w);
-                const float* ref = reinterpret_cast<const float*>(w.raw) + jr.ws_ref;
-                for (int a = g.lane; a < h->na; a += G) ro[jr.out_row + a] = wj[a] * (w.q[a] - ref[a]);
+                for (int a = g.lane; a < h->na; a += G) ro[jr.out_row + a] = jref_row(t, w, jr, w.q[a], a).r;
             }
         }
         float* S = ev.S;
@@ -236,7 +234,8 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 }
             for (int je = 0; je < h->njref; ++je) {
                 const JointRefEntry& jr = t.jref()[je];
-                for (int a = g.lane; a < h->na; a += G) Jo[(size_t)(jr.out_row + a) * D + boff + a] = t.at<float>(jr.o_w)[a];
+                for (int a = g.lane; a < h->na; a += G)
+                    Jo[(size_t)(jr.out_row + a) * D + boff + a] = jref_row(t, w, jr, w.q[a], a).js;
             }
         }
         for (int ci = 0; ci < h->ncoll; ++ci) {

@@ -569,7 +569,7 @@ int ik_server_add_type(IkServer* S, IkRobot* robot, int32_t floating_base, const
     T->slots = slots;
     T->params = *params;
     for (int i = 0; i < num_terms; ++i)
-        if (descs[i].kind == IK_TERM_JOINT_REF) {
+        if (descs[i].kind == IK_TERM_JOINT_REF || descs[i].kind == IK_TERM_VELOCITY_LIMIT) {
             delete T;
             return fail(IK_E_UNSUPPORTED, "term %d: joint-reference terms are not served (no per-request references)", i);
         } else if (descs[i].kind == IK_TERM_POSITION || descs[i].kind == IK_TERM_ROTATION || descs[i].kind == IK_TERM_FRAME) {

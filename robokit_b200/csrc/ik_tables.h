@@ -77,7 +77,8 @@ struct JointRefEntry {
     int32_t o_w;          // blob offset of the weights [na]
     int32_t ws_ref;       // workspace float offset of this problem's reference [na]
     const float* ref;     // device pointer [target_rows, na]
-    int64_t pad;
+    int32_t o_vlim;       // blob offset of the velocity limits [na]; 0 (the header) = a linear row
+    float dt;             // velocity rows: the time step
 };
 static_assert(sizeof(JointRefEntry) == 32, "JointRefEntry layout");
 

@@ -10,8 +10,8 @@ Everything between the host call and the result runs on the GPU: the spread
 (integrate + clamp kernels), one persistent solve launch per stage and one
 select launch between stages.  The term templates of the config (PositionTask,
 RotationTask, FrameTask with IKContext placeholders, PositionLimit,
-SelfCollisionTask, SmoothnessTask on IKContext.PREVIOUS_STATE, ConfigurationTask
-on IKContext.REST_Q) become concrete terms that read the solver's target,
+SelfCollisionTask, SmoothnessTask and VelocityLimitTask on
+IKContext.PREVIOUS_STATE, ConfigurationTask on IKContext.REST_Q) become concrete terms that read the solver's target,
 previous-state and rest buffers in place with the reference's broadcast rule
 (candidate c of target b reads row b).  With a previous state, each target keeps
 it where it scores no worse than the solve's result (helpers/ik/ik.py:257-289).
@@ -31,7 +31,7 @@ from ...opt.sampler import RobertsSampler
 from ...opt.var_values import VarKey, VarValues
 from ...robo.robot_state import RobotState
 from ...terms.dense import (ConfigurationTask, FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask,
-                            SmoothnessTask, _PoseTask)
+                            SmoothnessTask, VelocityLimitTask, _PoseTask)
 from ...terms.task import Context
 from .config import IKContext, IKSolverConfig
 
@@ -96,7 +96,7 @@ class IKSolver:
                 c = SelfCollisionTask(self.robot, t.weight, t.margin, max_active_pairs=t.max_active_pairs,
                                       filter_adjacent_links=t.filter_adjacent_links, pair_mode=t.pair_mode)
                 out.append(c)
-            elif isinstance(t, (SmoothnessTask, ConfigurationTask)) and t.robot is not None:
+            elif isinstance(t, (SmoothnessTask, ConfigurationTask, VelocityLimitTask)) and t.robot is not None:
                 out.append(t)  # built with a robot: passes as is
             elif isinstance(t, SmoothnessTask):
                 s = SmoothnessTask(self.robot, weight=t.weight, name=t.name)
@@ -105,6 +105,14 @@ class IKSolver:
                 elif t.prev_var is not None:
                     raise NotImplementedError("IKSolver smoothness templates take prev_var=IKContext.PREVIOUS_STATE")
                 out.append(s)
+            elif isinstance(t, VelocityLimitTask):
+                v = VelocityLimitTask(self.robot, dt=t.dt, velocity_limits=t.velocity_limits, weight=t.weight,
+                                      name=t.name)
+                if t.prev_state_var is IKContext.PREVIOUS_STATE:
+                    v.bind_previous(self._prev_q)
+                elif t.prev_state_var is not None:
+                    raise NotImplementedError("IKSolver velocity templates take prev_state_var=IKContext.PREVIOUS_STATE")
+                out.append(v)
             elif isinstance(t, ConfigurationTask):
                 c = ConfigurationTask(self.robot, rest_q=None if t.rest_q_arg is IKContext.REST_Q else t.rest_q_arg,
                                       weight=t.weight, name=t.name, mask=t.mask)

@@ -232,6 +232,13 @@ def _joint_limits(rec: JointRecord) -> Tuple[float, float]:
     return 0.0, 0.0
 
 
+def _joint_velocity_limit(rec: JointRecord) -> float:
+    # robo/robot_spec.py:373-384: fixed joints 0, unspecified 10
+    if rec.velocity is not None:
+        return rec.velocity
+    return 0.0 if rec.type == "fixed" else 10.0
+
+
 @dataclass
 class RobotSpec:
     """Kinematic tables of one robot (robo/robot_spec.py:44-139)."""
@@ -258,6 +265,15 @@ class RobotSpec:
     collision_spheres_link_indices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     self_collision_ignored_pairs: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
     robot_description: str = ""
+    joint_velocity_limits: Optional[np.ndarray] = None
+    actuated_joint_velocity_limits: Optional[np.ndarray] = None
+
+    def __post_init__(self):
+        # tables built without velocities (synthetic robots) get the reader's default of 10 per moving joint
+        if self.joint_velocity_limits is None:
+            self.joint_velocity_limits = np.where(np.asarray(self.joint_types) == 0, 0.0, 10.0)
+        if self.actuated_joint_velocity_limits is None:
+            self.actuated_joint_velocity_limits = np.full(len(self.actuated_joint_names), 10.0)
 
     # --- construction ---------------------------------------------------------
     @staticmethod
@@ -355,6 +371,8 @@ class RobotSpec:
             base_link_name=base_link_name,
             ee_link_names=list(ee_link_names),
             robot_description=description,
+            joint_velocity_limits=np.array([_joint_velocity_limit(j) for j in joints], np.float64),
+            actuated_joint_velocity_limits=np.array([_joint_velocity_limit(jmap[n]) for n in actuated], np.float64),
         )
 
     @staticmethod

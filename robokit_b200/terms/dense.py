@@ -5,7 +5,8 @@ PositionTask (terms/dense/position_task.py:18-272), RotationTask
 (terms/dense/frame_task.py:47-621), PositionLimit in "abs" mode
 (terms/dense/position_limit.py:185-573), the joint blocks of SmoothnessTask
 (terms/dense/smoothness_task.py:22-460) and ConfigurationTask
-(terms/dense/configuration_task.py:25-478), and SelfCollisionTask with sphere
+(terms/dense/configuration_task.py:25-478), VelocityLimitTask
+(terms/dense/velocity_limit_task.py:14-232), and SelfCollisionTask with sphere
 geometry (terms/dense/self_collision_task.py:593-1152).  Constructor
 signatures, defaults, residual_dim and set_weight / set_target follow the
 reference; the arithmetic runs in libb200ik.so.
@@ -432,6 +433,83 @@ class ConfigurationTask(_JointRefTask):
                 self._touch()
             return
         self._rest = new
+        self._touch()
+
+
+class VelocityLimitTask(_JointRefTask):
+    """Penalise joint speeds above their limits relative to a previous state,
+    w max(0, |q - q_prev| / dt - v_max) (velocity_limit_task.py:14-232).
+
+    ``velocity_limits`` defaults to the robot's actuated joint velocity limits and
+    ``weight`` to 1 per joint.  Without a previous state the term adds zero rows."""
+
+    def __init__(self, robot: Any = None, dt: Any = 1.0, prev_state_var: Any = None, velocity_limits: Any = None,
+                 weight: Optional[Union[float, Sequence[float]]] = None, name: str = ""):
+        if isinstance(dt, Context):
+            raise NotImplementedError("a helper-given dt is outside the IK hot path")
+        if not dt > 0:
+            raise ValueError("dt must be positive")
+        if isinstance(velocity_limits, Context):
+            raise NotImplementedError("helper-given velocity limits are outside the IK hot path")
+        self.name = name
+        self.dt = float(dt)
+        self.weight = weight
+        self.velocity_limits = None if velocity_limits is None else np.asarray(velocity_limits, np.float32)
+        self.robot = robot
+        self.prev_state_var = prev_state_var
+        self._prev_q: Any = None
+        if prev_state_var is not None and not isinstance(prev_state_var, Context):
+            self._prev_q = _ref_rows(prev_state_var.q, prev_state_var.spec.num_actuated_joints)
+            if isinstance(self._prev_q, N.DeviceArray):  # the reference clones the state (velocity_limit_task.py:39)
+                self._prev_q = self._prev_q.clone()
+
+    @property
+    def active(self) -> bool:
+        return self.weight is None or bool(np.any(self.weight))
+
+    def _joint_weights(self, na: int) -> np.ndarray:
+        w = np.ones(na, np.float32)
+        if self.weight is not None:
+            w[:] = self.weight
+        return w if self._prev_q is not None else np.zeros_like(w)
+
+    def _limits(self, var: Any) -> np.ndarray:
+        na = var.spec.num_actuated_joints
+        v = self.velocity_limits if self.velocity_limits is not None else var.spec.actuated_joint_velocity_limits
+        v = np.asarray(v, np.float32).reshape(-1)
+        if v.shape != (na,):
+            raise ValueError(f"velocity_limits has {v.shape[0]} entries for {na} actuated joints")
+        return v
+
+    def _reference(self, na: int) -> Any:
+        return self._prev_q if self._prev_q is not None else np.zeros((1, na), np.float32)
+
+    def native_desc(self, var: Any) -> Dict[str, Any]:
+        d = super().native_desc(var)
+        d.update(kind=N.IK_TERM_VELOCITY_LIMIT, dt=self.dt, velocity_limits=self._limits(var))
+        return d
+
+    def host_desc(self, var: Any) -> Dict[str, Any]:
+        d = super().host_desc(var)
+        d.update(kind=N.IK_TERM_VELOCITY_LIMIT, dt=self.dt, velocity_limits=self._limits(var))
+        return d
+
+    def set_weight(self, weight: Union[float, Sequence[float]]) -> None:
+        self.weight = weight
+        self._touch()
+
+    def bind_previous(self, prev_q: N.DeviceArray) -> None:
+        """Read the previous joints from `prev_q` [rows, na] in place from now on."""
+        self._prev_q = prev_q
+        self._touch()
+
+    def set_prev_state(self, prev_state: Any) -> None:
+        """Copy a new previous state in place; a new row count rebuilds (velocity_limit_task.py:81-88)."""
+        new = _ref_rows(prev_state.q, prev_state.spec.num_actuated_joints)
+        if isinstance(self._prev_q, N.DeviceArray) and self._prev_q.shape == new.shape:
+            self._prev_q.assign(new)
+            return
+        self._prev_q = new.clone() if isinstance(new, N.DeviceArray) else new
         self._touch()
 
 

@@ -147,6 +147,8 @@ def lower_terms(robot: Any, terms: List[ResidualTask], capacity: int, floating: 
         descs[i].link_pair_offsets = arr(d.get("link_pair_offsets"), np.int32)
         descs[i].num_sphere_pairs = d.get("num_sphere_pairs", 0)
         descs[i].sphere_pairs = arr(d.get("sphere_pairs"), np.int32)
+        descs[i].dt = d.get("dt", 0.0)
+        descs[i].velocity_limits = arr(d.get("velocity_limits"), np.float32)
     return descs
 
 

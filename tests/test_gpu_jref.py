@@ -9,7 +9,8 @@ from robokit_b200 import _native as N
 from robokit_b200.helpers.ik import IKContext, IKSolver, IKSolverConfig, presets
 from robokit_b200.opt import LMOptimizer, LMOptimizerConfig, VarKey, VarValues
 from robokit_b200.opt.population_solver import PopulationSolverConfig, Stage
-from robokit_b200.terms.dense import ConfigurationTask, PositionLimit, PositionTask, RotationTask, SmoothnessTask
+from robokit_b200.terms.dense import (ConfigurationTask, PositionLimit, PositionTask, RotationTask, SmoothnessTask,
+                                      VelocityLimitTask)
 
 pytestmark = pytest.mark.gpu
 
@@ -46,7 +47,8 @@ def test_joint_reference_rows_match_the_oracle(gpu, panda_spec, floating):
     terms = [PositionTask(robot, hand, tg, weight=3.0),
              SmoothnessTask(robot, prev_var=robot.state(prev), weight=w),
              ConfigurationTask(robot, rest_q=rest, weight=0.7, mask=(np.arange(na) % 2).astype(np.float32)),
-             ConfigurationTask(robot, rest_q="midrange", weight=0.25)]
+             ConfigurationTask(robot, rest_q="midrange", weight=0.25),
+             VelocityLimitTask(robot, dt=0.1, prev_state_var=robot.state(prev), weight=w[::-1].copy())]
     st = robot.state(q, base)
     vv = VarValues({VarKey.ROBOT: st})
     D = st.tangent_dim
@@ -63,8 +65,10 @@ def test_joint_reference_rows_match_the_oracle(gpu, panda_spec, floating):
                                       base)
     np.testing.assert_allclose(r.numpy(), ro, rtol=1e-5, atol=2e-6)
     np.testing.assert_allclose(J.numpy(), Jo, rtol=1e-5, atol=2e-6)
-    # the smoothness rows are exactly w (q - prev)
+    # the smoothness rows are exactly w (q - prev); some velocity rows are active, some not
     np.testing.assert_allclose(r.numpy()[:, 3:3 + na], w * (q - prev), rtol=1e-6, atol=1e-7)
+    vel = r.numpy()[:, -na:]
+    assert (vel > 0).any() and (vel == 0).any()
 
 
 @pytest.mark.parametrize("form", ["persistent", "plain"])
@@ -83,7 +87,9 @@ def test_lm_with_joint_references_matches_the_oracle(gpu, panda_arm_spec, form):
     prev = np.clip(qs + rng.normal(0, 0.1, qs.shape), lo, hi).astype(np.float32)
     terms = [PositionTask(robot, hand, T, weight=10.0), RotationTask(robot, hand, T, weight=5.0),
              PositionLimit(robot, 10.0), SmoothnessTask(robot, prev_var=robot.state(prev), weight=0.3),
-             ConfigurationTask(robot, rest_q="midrange", weight=0.05)]
+             ConfigurationTask(robot, rest_q="midrange", weight=0.05),
+             VelocityLimitTask(robot, dt=0.05, prev_state_var=robot.state(prev), velocity_limits=[2.0] * 7,
+                               weight=1.0)]
     opt = LMOptimizer(terms, LMOptimizerConfig(max_iter=30, lm_lambda=1e-2, lambda_factor=2.0,
                                                early_stopping_interval=0, form=form))
     st = robot.state(q0)

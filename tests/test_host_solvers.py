@@ -120,3 +120,32 @@ def test_joint_reference_terms_host_side(panda_spec):
     assert [type(t).__name__ for t in presets.smooth.terms] == ["PositionTask", "RotationTask", "PositionLimit",
                                                                 "SmoothnessTask"]
     assert type(presets.single_candidate.terms[-1]).__name__ == "SmoothnessTask"
+
+
+def test_velocity_limit_term_host_side(panda_spec):
+    from robokit_b200.terms.dense import VelocityLimitTask
+
+    class _Robot:
+        spec = panda_spec
+
+    class _V:
+        spec, batch_size, has_floating_base = panda_spec, 4, False
+
+    na = panda_spec.num_actuated_joints
+    v = VelocityLimitTask(_Robot(), dt=0.02)
+    d = v.host_desc(_V)
+    assert d["kind"] == N.IK_TERM_VELOCITY_LIMIT and d["dt"] == 0.02 and v.residual_dim == na
+    np.testing.assert_allclose(d["velocity_limits"], panda_spec.actuated_joint_velocity_limits)
+    assert not np.any(d["weights"])  # no previous state: zero rows
+    with pytest.raises(ValueError):
+        VelocityLimitTask(_Robot(), dt=0.0)
+    with pytest.raises(ValueError):
+        VelocityLimitTask(_Robot(), velocity_limits=[1.0, 2.0]).host_desc(_V)
+    # the URDF reader's velocity limits: the file's value, 0 for fixed joints without one, else 10
+    from robokit_b200.robo.robot_spec import JointRecord, RobotSpec
+
+    recs = [JointRecord("a", "revolute", "l0", "l1", velocity=3.0), JointRecord("b", "continuous", "l1", "l2"),
+            JointRecord("c", "fixed", "l2", "l3")]
+    s = RobotSpec.from_records("r", ["l0", "l1", "l2", "l3"], recs)
+    np.testing.assert_array_equal(s.joint_velocity_limits, [3.0, 10.0, 0.0])
+    np.testing.assert_array_equal(s.actuated_joint_velocity_limits, [3.0, 10.0])

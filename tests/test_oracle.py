@@ -248,3 +248,27 @@ def test_oracle_joint_reference_term(panda_spec):
         expect = np.zeros((B, na, boff + na))
         expect[:, np.arange(na), boff + np.arange(na)] = w
         np.testing.assert_array_equal(J, expect)
+
+
+def test_oracle_velocity_limit_term(panda_spec):
+    """Velocity rows: qd = (q - prev) / dt, r = w max(0, |qd| - vmax), J = w sign(qd) / dt where active."""
+    spec = panda_spec
+    rob = oracle.Robot.from_spec(spec)
+    na = spec.num_actuated_joints
+    rng = np.random.default_rng(9)
+    B = 5
+    prev = rng.normal(0, 0.5, (1, na)).astype(np.float32)  # one row for every problem
+    q = (prev + rng.normal(0, 0.3, (B, na))).astype(np.float32)
+    dt = 0.1
+    vmax = np.full(na, 2.0, np.float32)
+    w = np.linspace(0.5, 1.5, na).astype(np.float32)
+    terms = oracle.Terms([dict(kind=7, weights=w, targets=prev, target_rows=1, dt=dt, velocity_limits=vmax)])
+    assert oracle.residual_dim(rob, terms) == na
+    r, J = oracle.residual_jacobian(rob, terms, q)
+    qd = (q.astype(np.float64) - prev) / np.float32(dt)
+    act = np.abs(qd) > vmax
+    assert act.any() and (~act).any()
+    np.testing.assert_allclose(r, np.where(act, w * (np.abs(qd) - vmax), 0.0), rtol=1e-12, atol=1e-12)
+    expect = np.zeros((B, na, na))
+    expect[:, np.arange(na), np.arange(na)] = np.where(act, w * np.sign(qd) / np.float32(dt), 0.0)
+    np.testing.assert_allclose(J, expect, rtol=1e-12, atol=0)
