@@ -702,7 +702,10 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
             const V3 wc = pose_apply(P, V3{c[0], c[1], c[2]});
             *reinterpret_cast<float4*>(w.sph() + 4 * s) = make_float4(wc.x, wc.y, wc.z, c[3]);
         }
-        {
+        bool need_lbw = false;  // link bounding spheres feed the pruned scans only
+        for (int ci = 0; ci < h->ncoll; ++ci)
+            need_lbw = need_lbw || t.coll()[ci].mode == 0 || !pairs_by_mask<G>(t.coll()[ci]);
+        if (need_lbw) {
             for (int l = g.lane; l < h->nl; l += G) {
                 const Pose P = link_pose(t, Tj, base, l);
                 const float* c = t.lbound() + 4 * l;
@@ -1057,8 +1060,8 @@ __device__ __forceinline__ void group_collision_rows(const Group<G>& g, const Ta
         const float pen = ce.margin - surf;
         float val = 0.f;
         if (pen > 0.f) {
-            const float den = fmaxf(1e-8f, dist);
-            const V3 n{diff.x / den, diff.y / den, diff.z / den};
+            const float inv = 1.f / fmaxf(1e-8f, dist);
+            const V3 n{diff.x * inv, diff.y * inv, diff.z * inv};
             val = -ce.weight * collision_column(t, S, base, c, t.sphlink()[si], t.sphlink()[sj], ci, cj, n);
         }
         w.Jc()[r * Dp + c] = val;
@@ -1229,36 +1232,34 @@ constexpr int kSmallD = 8;  // systems up to this size are factorised in registe
 
 __host__ __device__ constexpr int ctri(int i, int j) { return (i * (i + 1)) / 2 + j; }
 
-// D <= kSmallD: every lane factorises the (identity-padded) system in FP64
-// registers — left-looking Cholesky, forward and back substitution fully
-// unrolled — so the solve needs no shared memory and no synchronisation; all
-// lanes hold the same step.
-template <int G>
-__device__ __forceinline__ bool group_small_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
-                                  double& pred, double& dnorm) {
-    const int D = t.h->D, T = t.h->T;
+// D <= kSmallD: every lane factorises the system in FP64 registers at its
+// exact size N = D — left-looking Cholesky, forward and back substitution
+// fully unrolled — so the solve needs no shared memory and no
+// synchronisation; all lanes hold the same step.
+template <int G, int N>
+__device__ __forceinline__ bool group_small_solve_n(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp,
+                                                    float lambda_f, double& pred, double& dnorm) {
+    const int D = N, T = t.h->T;
     const double lam = (double)lambda_f;
-    double a[ctri(kSmallD, 0)];
-    double y[kSmallD];
-    sfor<kSmallD>([&](auto I) {
+    double a[ctri(N, 0)];
+    double y[N];
+    sfor<N>([&](auto I) {
         constexpr int i = decltype(I)::value;
         sfor<i + 1>([&](auto J) {
             constexpr int j = decltype(J)::value;
-            double v = (i == j) ? 1.0 : 0.0;
-            if (i < D) v = (double)Hp[ctri(i, j)] + ((i == j) ? lam : 0.0);
-            a[ctri(i, j)] = v;
+            a[ctri(i, j)] = (double)Hp[ctri(i, j)] + ((i == j) ? lam : 0.0);
         });
-        y[i] = (i < D) ? -(double)Hp[T + i] : 0.0;
+        y[i] = -(double)Hp[T + i];
     });
     bool ok = true;
-    sfor<kSmallD>([&](auto K) {
+    sfor<N>([&](auto K) {
         constexpr int k = decltype(K)::value;
         double s = a[ctri(k, k)];
         sfor<k>([&](auto M) { constexpr int m = decltype(M)::value; s -= a[ctri(k, m)] * a[ctri(k, m)]; });
         ok = ok && (s > 0.0);
         const double inv = rsqrt(s);
         a[ctri(k, k)] = inv;
-        sfor<kSmallD - k - 1>([&](auto I0) {
+        sfor<N - k - 1>([&](auto I0) {
             constexpr int i = k + 1 + decltype(I0)::value;
             double v = a[ctri(i, k)];
             sfor<k>([&](auto M) { constexpr int m = decltype(M)::value; v -= a[ctri(i, m)] * a[ctri(k, m)]; });
@@ -1272,37 +1273,50 @@ __device__ __forceinline__ bool group_small_solve(const Group<G>& g, const Tabs&
         g.sync();
         return false;
     }
-    sfor<kSmallD>([&](auto I) {
+    sfor<N>([&](auto I) {
         constexpr int i = decltype(I)::value;
         double v = y[i];
         sfor<i>([&](auto M) { constexpr int m = decltype(M)::value; v -= a[ctri(i, m)] * y[m]; });
         y[i] = v * a[ctri(i, i)];
     });
-    sfor<kSmallD>([&](auto I0) {
-        constexpr int i = kSmallD - 1 - decltype(I0)::value;
+    sfor<N>([&](auto I0) {
+        constexpr int i = N - 1 - decltype(I0)::value;
         double v = y[i];
-        sfor<kSmallD - 1 - i>([&](auto M0) {
+        sfor<N - 1 - i>([&](auto M0) {
             constexpr int m = i + 1 + decltype(M0)::value;
             v -= a[ctri(m, i)] * y[m];
         });
         y[i] = v * a[ctri(i, i)];
     });
     double pp = 0.0, nn = 0.0;
-    sfor<kSmallD>([&](auto I) {
+    sfor<N>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        if (i < D) {
-            pp += y[i] * (lam * y[i] - (double)Hp[T + i]);
-            nn += y[i] * y[i];
-        }
+        pp += y[i] * (lam * y[i] - (double)Hp[T + i]);
+        nn += y[i] * y[i];
     });
     pred = 0.5 * pp;
     dnorm = sqrt(nn);
-    sfor<kSmallD>([&](auto I) {
+    sfor<N>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        if (i < D && (i % G) == g.lane) w.d32()[i] = (float)y[i];
+        if ((i % G) == g.lane) w.d32()[i] = (float)y[i];
     });
     g.sync();
     return true;
+}
+
+template <int G>
+__device__ __forceinline__ bool group_small_solve(const Group<G>& g, const Tabs& t, Ws& w, const float* Hp, float lambda_f,
+                                                  double& pred, double& dnorm) {
+    switch (t.h->D) {
+        case 1: return group_small_solve_n<G, 1>(g, t, w, Hp, lambda_f, pred, dnorm);
+        case 2: return group_small_solve_n<G, 2>(g, t, w, Hp, lambda_f, pred, dnorm);
+        case 3: return group_small_solve_n<G, 3>(g, t, w, Hp, lambda_f, pred, dnorm);
+        case 4: return group_small_solve_n<G, 4>(g, t, w, Hp, lambda_f, pred, dnorm);
+        case 5: return group_small_solve_n<G, 5>(g, t, w, Hp, lambda_f, pred, dnorm);
+        case 6: return group_small_solve_n<G, 6>(g, t, w, Hp, lambda_f, pred, dnorm);
+        case 7: return group_small_solve_n<G, 7>(g, t, w, Hp, lambda_f, pred, dnorm);
+        default: return group_small_solve_n<G, 8>(g, t, w, Hp, lambda_f, pred, dnorm);
+    }
 }
 
 // D > kSmallD: blocked right-looking factorisation in shared memory.  Per
