@@ -66,6 +66,27 @@ extern "C" {
 #define IK_TERM_VELOCITY_LIMIT 7 /* w_a max(0, |q_a - prev_a| / dt - vmax_a), one row per actuated joint:
                                     VelocityLimitTask (velocity_limit_task.py:14); weights [na];
                                     d_targets = previous joints [target_rows, na]; dt, velocity_limits */
+#define IK_TERM_SCENE_COLLISION 8 /* terms/dense/scene_collision_task.py:276 with primitive geometry
+                                     (geom/geoms.py:372-500): one row per queried robot sphere,
+                                     w * penalty(sdf(centre) - radius); weights [num_query_spheres] */
+
+/* scene-collision penalties (terms/sphere_collision_kernels.py:17-41) */
+#define IK_PENALTY_SMOOTH 0
+#define IK_PENALTY_PLAIN 1
+#define IK_PENALTY_SURFACE_DISTANCE 2
+
+/* scene primitives (geom/geoms.py:372-500, geom/sdf_kernels.py:223-344) and the
+ * host record of one primitive: IK_GEOM_FLOATS floats
+ *   [0] type IK_GEOM_*, [1] scene index, [2] uniform scale (1 = none), [3] 0,
+ *   [4..7] parameters: box half extents (x, y, z); sphere radius; plane none;
+ *          capsule radius, half height (axis local z),
+ *   [8..14] pose [x y z qw qx qy qz] of the primitive in the world, [15] 0. */
+#define IK_GEOM_BOX 0
+#define IK_GEOM_SPHERE 1
+#define IK_GEOM_PLANE 2
+#define IK_GEOM_CAPSULE 3
+#define IK_GEOM_FLOATS 16
+#define IK_SCENE_MAX_TERMS 8
 
 /* self-collision pair modes */
 #define IK_PAIRS_SLOTS 0 /* reference: <= K link pairs, most penetrating sphere pair each */
@@ -130,6 +151,19 @@ typedef struct IkTermDesc {
     /* velocity limit */
     float dt;                         /* > 0                                              */
     const float* velocity_limits;     /* host [na]                                        */
+    /* scene collision (margin above is the activation distance) */
+    int32_t num_query_spheres;        /* robot spheres queried, one row each               */
+    const int32_t* query_spheres;     /* host [num_query_spheres] sphere indices           */
+    int32_t num_geoms;
+    const float* geoms;               /* host [num_geoms * IK_GEOM_FLOATS], query order: a point
+                                         keeps the first primitive of strictly least distance */
+    int32_t num_scenes;
+    int32_t penalty;                  /* IK_PENALTY_*                                       */
+    int32_t residual_sqrt;            /* residual_mode "sqrt_abs": sqrt(penalty + eps)      */
+    float residual_eps;
+    const int32_t* d_scene_indices;   /* device [scene_rows]: scene of problem row b / max(1,
+                                         batch / scene_rows); NULL = scene 0 for all        */
+    int32_t scene_rows;
 } IkTermDesc;
 
 /* LMOptimizerConfig (opt/lm_optimizer.py:503-523) + OptimizerConfig

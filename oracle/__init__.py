@@ -74,6 +74,16 @@ class OrTerm(ctypes.Structure):
         ("sphere_pairs", ctypes.c_void_p),
         ("dt", ctypes.c_float),
         ("velocity_limits", ctypes.c_void_p),
+        ("num_query_spheres", ctypes.c_int32),
+        ("query_spheres", ctypes.c_void_p),
+        ("num_geoms", ctypes.c_int32),
+        ("geoms", ctypes.c_void_p),
+        ("num_scenes", ctypes.c_int32),
+        ("penalty", ctypes.c_int32),
+        ("residual_sqrt", ctypes.c_int32),
+        ("residual_eps", ctypes.c_float),
+        ("scene_indices", ctypes.c_void_p),
+        ("scene_rows", ctypes.c_int32),
     ]
 
 
@@ -155,6 +165,19 @@ class Terms:
             arr[i].sphere_pairs = keep(t.get("sphere_pairs"), np.int32)
             arr[i].dt = t.get("dt", 0.0)
             arr[i].velocity_limits = keep(t.get("velocity_limits"), np.float32)
+            qs = t.get("query_spheres")
+            arr[i].num_query_spheres = 0 if qs is None else len(qs)
+            arr[i].query_spheres = keep(qs, np.int32)
+            gm = t.get("geoms")
+            arr[i].num_geoms = 0 if gm is None else int(np.asarray(gm).size // 16)
+            arr[i].geoms = keep(gm, np.float32) if gm is not None and np.asarray(gm).size else None
+            arr[i].num_scenes = t.get("num_scenes", 0)
+            arr[i].penalty = t.get("penalty", 0)
+            arr[i].residual_sqrt = int(bool(t.get("residual_sqrt", 0)))
+            arr[i].residual_eps = t.get("residual_eps", 0.0)
+            si = t.get("scene_indices")
+            arr[i].scene_indices = keep(si, np.int32)
+            arr[i].scene_rows = 0 if si is None else int(np.asarray(si).size)
         self.arr = arr
         self.n = len(terms)
 

@@ -421,6 +421,91 @@ static void collision_row(const OrRobot* r, const Kin* K, int floating, const do
     }
 }
 
+/* Scene SDF at world point p over the primitives of scene `sid` in query order:
+ * the first of strictly least signed distance and its world normal
+ * (geom/sdf_kernels.py:223-344); 1e6 and a zero normal for an empty scene. */
+static double scene_sdf(const OrTerm* t, int sid, const double* p, double* n_out) {
+    double best = 1.0e6;
+    n_out[0] = n_out[1] = n_out[2] = 0.0;
+    for (int e = 0; e < t->num_geoms; ++e) {
+        const float* g = t->geoms + (size_t)e * 16;
+        if ((int)g[1] != sid) continue;
+        const int type = (int)g[0];
+        const double s = g[2];
+        P7 P;
+        P.t[0] = g[8], P.t[1] = g[9], P.t[2] = g[10];
+        double qn = sqrt((double)g[11] * g[11] + (double)g[12] * g[12] + (double)g[13] * g[13] + (double)g[14] * g[14]);
+        P.q[0] = g[11] / qn, P.q[1] = g[12] / qn, P.q[2] = g[13] / qn, P.q[3] = g[14] / qn;
+        const P7 Pi = inverse(&P);
+        double ql[3];
+        qrot(Pi.q, p, ql);
+        for (int k = 0; k < 3; ++k) ql[k] = (ql[k] + Pi.t[k]) / s;
+        double un = 0.0, nl[3] = {0.0, 0.0, 1.0};
+        if (type == 0) { /* box */
+            const double he[3] = {g[4], g[5], g[6]};
+            double qv[3], qp[3];
+            for (int k = 0; k < 3; ++k) {
+                qv[k] = fabs(ql[k]) - he[k];
+                qp[k] = qv[k] > 0 ? qv[k] : 0.0;
+            }
+            const double qmax = fmax(fmax(qv[0], qv[1]), qv[2]);
+            un = sqrt(dot3(qp, qp)) + (qmax < 0 ? qmax : 0.0);
+            if (qmax < 0) {
+                int ax = (qv[0] >= qv[1] && qv[0] >= qv[2]) ? 0 : (qv[1] >= qv[2] ? 1 : 2);
+                nl[0] = nl[1] = nl[2] = 0.0;
+                nl[ax] = ql[ax] < 0 ? -1.0 : 1.0;
+            } else {
+                double d[3];
+                for (int k = 0; k < 3; ++k) d[k] = ql[k] - fmin(fmax(ql[k], -he[k]), he[k]);
+                const double dl = sqrt(dot3(d, d));
+                if (dl > 1e-10)
+                    for (int k = 0; k < 3; ++k) nl[k] = d[k] / dl;
+            }
+        } else if (type == 1) { /* sphere */
+            const double l = sqrt(dot3(ql, ql));
+            un = l - g[4];
+            if (l > 1e-10)
+                for (int k = 0; k < 3; ++k) nl[k] = ql[k] / l;
+            else
+                nl[0] = 1.0, nl[1] = nl[2] = 0.0;
+        } else if (type == 2) { /* plane: local z */
+            un = ql[2];
+        } else { /* capsule along local z */
+            const double tz = fmin(fmax(ql[2], -(double)g[5]), (double)g[5]);
+            const double d[3] = {ql[0], ql[1], ql[2] - tz};
+            const double l = sqrt(dot3(d, d));
+            un = l - g[4];
+            if (l > 1e-10)
+                for (int k = 0; k < 3; ++k) nl[k] = d[k] / l;
+            else
+                nl[0] = 1.0, nl[1] = nl[2] = 0.0;
+        }
+        const double dist = un * s;
+        if (dist < best) {
+            best = dist;
+            qrot(P.q, nl, n_out);
+        }
+    }
+    return best;
+}
+
+/* penalty and its derivative, terms/sphere_collision_kernels.py:17-41 */
+static void scene_penalty(double sd, double margin, int mode, double* pen, double* dpen) {
+    *pen = *dpen = 0.0;
+    if (mode == 2) {
+        *pen = fabs(sd);
+        *dpen = sd > 0 ? 1.0 : (sd < 0 ? -1.0 : 0.0);
+    } else if (mode == 1) {
+        if (sd < margin) *pen = margin - sd, *dpen = -1.0;
+    } else if (sd < 0) {
+        *pen = 0.5 * margin - sd, *dpen = -1.0;
+    } else if (sd <= margin) {
+        const double inv = 1.0 / (margin + 1e-6);
+        *pen = 0.5 * inv * (sd - margin) * (sd - margin);
+        *dpen = inv * (sd - margin);
+    }
+}
+
 int or_residual_dim(const OrRobot* r, const OrTerm* terms, int32_t nterms) {
     int R = 0;
     for (int i = 0; i < nterms; ++i) {
@@ -431,6 +516,8 @@ int or_residual_dim(const OrRobot* r, const OrTerm* terms, int32_t nterms) {
             R += 6 * t->num_frames;
         else if (t->kind == 3 || t->kind == 6 || t->kind == 7)
             R += r->na;
+        else if (t->kind == 8)
+            R += t->num_query_spheres;
         else if (t->kind == 4)
             R += t->pair_mode == 0 ? t->max_active_pairs : t->num_sphere_pairs;
     }
@@ -589,6 +676,50 @@ static void eval_terms(const OrRobot* r, const OrTerm* terms, int nterms, int fl
                 }
             }
             row += r->na;
+        } else if (t->kind == 8) {
+            /* scene_collision_task.py:34-82, 550-647 with primitive geometry */
+            if (!have_C) {
+                world_spheres(r, K, C);
+                have_C = 1;
+            }
+            int sid = 0;
+            if (t->scene_rows > 0 && t->scene_indices) {
+                int rep = B / t->scene_rows;
+                if (rep < 1) rep = 1;
+                int rr = b / rep;
+                if (rr > t->scene_rows - 1) rr = t->scene_rows - 1;
+                sid = t->scene_indices[rr];
+            }
+            if (sid < 0) sid = 0;
+            if (sid > t->num_scenes - 1) sid = t->num_scenes - 1;
+            for (int k = 0; k < t->num_query_spheres; ++k) {
+                const int s = t->query_spheres[k];
+                const double* c = C + 3 * s;
+                double n[3];
+                const double sd = scene_sdf(t, sid, c, n) - r->sphere_radii[s];
+                double pen, dpen;
+                scene_penalty(sd, t->margin, t->penalty, &pen, &dpen);
+                double rv = pen, sc = dpen;
+                if (t->residual_sqrt) {
+                    if (pen > 0) sc *= 0.5 / sqrt(pen + t->residual_eps);
+                    rv = sqrt(pen + t->residual_eps);
+                }
+                res[row + k] = t->weights[k] * rv;
+                if (J) {
+                    double* jr = J + (size_t)(row + k) * D;
+                    const int act = t->penalty == 2 || sd <= t->margin;
+                    for (int col = 0; col < D; ++col) {
+                        jr[col] = 0.0;
+                        if (!act) continue;
+                        double v[3], w[3], x[3];
+                        column_twist(r, K, floating, col, r->sphere_links[s], v, w);
+                        cross3(w, c, x);
+                        const double pc[3] = {v[0] + x[0], v[1] + x[1], v[2] + x[2]};
+                        jr[col] = t->weights[k] * sc * dot3(n, pc);
+                    }
+                }
+            }
+            row += t->num_query_spheres;
         } else if (t->kind == 4) {
             if (!have_C) {
                 world_spheres(r, K, C);

@@ -37,7 +37,7 @@ typedef struct OrRobot {
 typedef struct OrTerm {
     int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision, 5 frame ("log"),
                      6 joint reference (smoothness / configuration, joints only),
-                     7 velocity limit */
+                     7 velocity limit, 8 scene collision over primitives */
     int32_t num_frames;
     const int32_t* frame_links;
     const float* weights;
@@ -53,6 +53,17 @@ typedef struct OrTerm {
     const int32_t* sphere_pairs;
     float dt;                     /* kind 7 */
     const float* velocity_limits; /* kind 7: [na] */
+    /* kind 8 (margin above is the activation distance) */
+    int32_t num_query_spheres;
+    const int32_t* query_spheres;
+    int32_t num_geoms;
+    const float* geoms;           /* [num_geoms * 16]: type, scene, scale, 0, params[4], pose[7], 0 */
+    int32_t num_scenes;
+    int32_t penalty;              /* 0 smooth, 1 plain, 2 surface distance */
+    int32_t residual_sqrt;
+    float residual_eps;
+    const int32_t* scene_indices; /* host [scene_rows] or NULL */
+    int32_t scene_rows;
 } OrTerm;
 
 typedef struct OrParams {

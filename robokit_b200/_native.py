@@ -38,6 +38,10 @@ IK_TERM_SELF_COLLISION = 4
 IK_TERM_FRAME = 5
 IK_TERM_JOINT_REF = 6
 IK_TERM_VELOCITY_LIMIT = 7
+IK_TERM_SCENE_COLLISION = 8
+IK_PENALTY_SMOOTH, IK_PENALTY_PLAIN, IK_PENALTY_SURFACE_DISTANCE = 0, 1, 2
+IK_GEOM_BOX, IK_GEOM_SPHERE, IK_GEOM_PLANE, IK_GEOM_CAPSULE = 0, 1, 2, 3
+IK_GEOM_FLOATS = 16
 
 IK_PAIRS_SLOTS = 0
 IK_PAIRS_ALL = 1
@@ -108,6 +112,16 @@ class IkTermDesc(ctypes.Structure):
         ("sphere_pairs", _vp),
         ("dt", ctypes.c_float),
         ("velocity_limits", _vp),
+        ("num_query_spheres", ctypes.c_int32),
+        ("query_spheres", _vp),
+        ("num_geoms", ctypes.c_int32),
+        ("geoms", _vp),
+        ("num_scenes", ctypes.c_int32),
+        ("penalty", ctypes.c_int32),
+        ("residual_sqrt", ctypes.c_int32),
+        ("residual_eps", ctypes.c_float),
+        ("d_scene_indices", _vp),
+        ("scene_rows", ctypes.c_int32),
     ]
 
 

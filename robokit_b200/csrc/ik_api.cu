@@ -149,7 +149,8 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_base = take(h->base_off ? 32 : 0);
     h->w_basep = take(h->base_off ? 32 : 0);
     h->w_d32 = take(D * 4);
-    h->w_misc = take((8 + h->ncoll) * 4);  // [8 + ci]: filled slots of collision term ci
+    h->w_misc = take((8 + h->ncoll + h->nscene) * 4);  // [8 + ci]: filled slots of collision term ci, then
+                                                       // the scene index of each scene term
     const int slots_off = take(ncoll_slots_bytes);
     h->ws_bytes = off;
     return slots_off;
@@ -594,6 +595,28 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         }
         jref.push_back(e);
     }
+    // scene-collision terms
+    std::vector<SceneEntry> scene;
+    for (size_t ti = 0; ti < terms.size(); ++ti) {
+        const TermHost& th = terms[ti];
+        if (th.d.kind != IK_TERM_SCENE_COLLISION) continue;
+        SceneEntry e;
+        std::memset(&e, 0, sizeof(e));
+        e.out_row = th.row;
+        e.nq = (int)th.qsph.size();
+        e.o_q = b.addv(th.qsph);
+        e.o_w = b.addv(th.weights);
+        e.o_elem = b.addv(th.selem);
+        e.o_off = b.addv(th.soff);
+        e.nscenes = th.d.num_scenes;
+        e.penalty = th.d.penalty;
+        e.use_sqrt = th.d.residual_sqrt ? 1 : 0;
+        e.margin = th.d.margin;
+        e.eps = th.d.residual_eps;
+        e.scene_rows = th.d.d_scene_indices ? th.d.scene_rows : 0;
+        e.scene_idx = th.d.d_scene_indices;
+        scene.push_back(e);
+    }
     h = b.hdr();
     h->npose = (int)pose.size();
     h->pose_rows = pose_rows;
@@ -635,6 +658,10 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     const int o_coll = b.add(coll.data(), coll.size() * sizeof(CollEntry));
     b.hdr()->o_coll = o_coll;
     const int o_jref = b.add(jref.data(), jref.size() * sizeof(JointRefEntry));
+    if (scene.size() > IK_SCENE_MAX_TERMS) return fail(IK_E_UNSUPPORTED, "more than %d scene-collision terms", IK_SCENE_MAX_TERMS);
+    const int o_scene = b.add(scene.data(), scene.size() * sizeof(SceneEntry));
+    b.hdr()->o_scene = o_scene;
+    b.hdr()->nscene = (int)scene.size();
     b.hdr()->o_jref = o_jref;
     o = b.addv(limw);
     b.hdr()->o_limw = o;
@@ -648,11 +675,13 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     h = b.hdr();
     h->ncoll = (int)coll.size();
     h->max_slots = max_slots;
-    const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0, h->ncoll > 0);
+    const int slots_off = layout_workspace(h, h->npose, slot_bytes, h->ncoll > 0 || h->nscene > 0, h->ncoll > 0);
     CollEntry* ce = reinterpret_cast<CollEntry*>(b.buf.data() + o_coll);
     for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
     JointRefEntry* je = reinterpret_cast<JointRefEntry*>(b.buf.data() + o_jref);
     for (size_t i = 0; i < jref.size(); ++i) je[i].ws_ref = h->w_jref / 4 + (int)i * h->na;
+    SceneEntry* se = reinterpret_cast<SceneEntry*>(b.buf.data() + o_scene);
+    for (size_t i = 0; i < scene.size(); ++i) se[i].misc = 8 + h->ncoll + (int)i;
     // lane-per-problem layout: small systems with all-pairs collision terms only
     {
         int off = 0;
@@ -671,7 +700,7 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         h->t_qp = take(std::max(h->na, 1));
         h->t_base = take(h->base_off ? 7 : 0);
         h->t_basep = take(h->base_off ? 7 : 0);
-        bool ok = h->D <= kSmallD && h->nframe == 0 && h->njref == 0;
+        bool ok = h->D <= kSmallD && h->nframe == 0 && h->njref == 0 && h->nscene == 0;
         for (size_t i = 0; i < coll.size(); ++i) {
             if (ce[i].mode != IK_PAIRS_ALL) ok = false;
             ce[i].t_mask = take((ce[i].nsp + 31) / 32);
@@ -686,6 +715,65 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     out.D = h->D;
     out.R = R;
     out.E = h->E;
+    return IK_OK;
+}
+
+// Check a scene-collision term and turn its primitives into device records:
+// inverse pose rows [R^T | -R^T t], parameters, (type, scale), stably sorted by
+// scene so that each scene's primitives keep their query order.
+static int scene_records(const RobotHost& r, const IkTermDesc& d, int i, TermHost& th) {
+    if (r.ns < 1) return fail(IK_E_INVALID, "term %d: robot has no collision spheres", i);
+    if (d.num_query_spheres < 1 || !d.query_spheres || !d.weights)
+        return fail(IK_E_INVALID, "term %d: scene collision needs query spheres and weights", i);
+    if (d.num_scenes < 1) return fail(IK_E_INVALID, "term %d: num_scenes %d < 1", i, d.num_scenes);
+    if (d.num_geoms < 0 || (d.num_geoms > 0 && !d.geoms)) return fail(IK_E_INVALID, "term %d: geoms are NULL", i);
+    if (d.penalty < IK_PENALTY_SMOOTH || d.penalty > IK_PENALTY_SURFACE_DISTANCE)
+        return fail(IK_E_INVALID, "Unsupported penalty: %d", d.penalty);
+    if (d.scene_rows < 0 || (d.scene_rows > 0 && !d.d_scene_indices))
+        return fail(IK_E_INVALID, "term %d: scene indices are NULL", i);
+    th.qsph.assign(d.query_spheres, d.query_spheres + d.num_query_spheres);
+    for (int s : th.qsph)
+        if (s < 0 || s >= r.ns) return fail(IK_E_INVALID, "sphere_indices contains out-of-range indices.");
+    std::vector<int> order(d.num_geoms);
+    for (int k = 0; k < d.num_geoms; ++k) {
+        const float* g = d.geoms + (size_t)k * IK_GEOM_FLOATS;
+        const int type = (int)g[0], scene = (int)g[1];
+        if (g[0] != (float)type || type < IK_GEOM_BOX || type > IK_GEOM_CAPSULE)
+            return fail(IK_E_INVALID, "term %d: geom %d has type %g", i, k, g[0]);
+        if (g[1] != (float)scene || scene < 0 || scene >= d.num_scenes)
+            return fail(IK_E_INVALID, "term %d: geom %d in scene %g of %d", i, k, g[1], d.num_scenes);
+        if (!(g[2] > 0.f)) return fail(IK_E_INVALID, "term %d: geom %d scale %g", i, k, g[2]);
+        order[k] = k;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return d.geoms[(size_t)a * IK_GEOM_FLOATS + 1] < d.geoms[(size_t)b * IK_GEOM_FLOATS + 1]; });
+    th.soff.assign(d.num_scenes + 1, 0);
+    th.selem.clear();
+    for (int k : order) {
+        const float* g = d.geoms + (size_t)k * IK_GEOM_FLOATS;
+        th.soff[(int)g[1] + 1] += 1;
+        double qw = g[11], qx = g[12], qy = g[13], qz = g[14];
+        const double n = std::sqrt(qw * qw + qx * qx + qy * qy + qz * qz);
+        if (!(n > 0.0)) return fail(IK_E_INVALID, "term %d: geom %d has a zero quaternion", i, k);
+        qw /= n, qx /= n, qy /= n, qz /= n;
+        const double R[3][3] = {{1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy)},
+                                {2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx)},
+                                {2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)}};
+        const double t[3] = {g[8], g[9], g[10]};
+        for (int row = 0; row < 3; ++row) {  // row `row` of R^T is column `row` of R
+            const double c0 = R[0][row], c1 = R[1][row], c2 = R[2][row];
+            th.selem.push_back((float)c0);
+            th.selem.push_back((float)c1);
+            th.selem.push_back((float)c2);
+            th.selem.push_back((float)-(c0 * t[0] + c1 * t[1] + c2 * t[2]));
+        }
+        for (int k2 = 0; k2 < 4; ++k2) th.selem.push_back(g[4 + k2]);
+        th.selem.push_back(g[0]);
+        th.selem.push_back(g[2]);
+        th.selem.push_back(0.f);
+        th.selem.push_back(0.f);
+    }
+    for (int s = 0; s < d.num_scenes; ++s) th.soff[s + 1] += th.soff[s];
     return IK_OK;
 }
 
@@ -715,6 +803,11 @@ int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc*
             const int per = d.kind == IK_TERM_FRAME ? 2 : 3;
             th.weights.assign(d.weights, d.weights + per * d.num_frames);
             th.rows = (d.kind == IK_TERM_FRAME ? 6 : 3) * d.num_frames;
+        } else if (d.kind == IK_TERM_SCENE_COLLISION) {
+            int rc = scene_records(r, d, i, th);
+            if (rc) return rc;
+            th.weights.assign(d.weights, d.weights + d.num_query_spheres);
+            th.rows = d.num_query_spheres;
         } else if (d.kind == IK_TERM_JOINT_REF || d.kind == IK_TERM_VELOCITY_LIMIT) {
             if (!d.weights && r.na > 0) return fail(IK_E_INVALID, "term %d: joint weights are NULL", i);
             if (!d.d_targets) return fail(IK_E_INVALID, "term %d: joint-reference term needs a reference array", i);
@@ -1033,8 +1126,8 @@ int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, 
     const int G = problem_group(P);
     const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
     const TabHeader* th = reinterpret_cast<const TabHeader*>(P->blob.data());
-    if (th->nframe == 0 && th->njref == 0) {
-        // no frame or joint-reference entries: the kernel without those paths (a smaller instruction footprint)
+    if (th->nframe == 0 && th->njref == 0 && th->nscene == 0) {
+        // no frame, joint-reference or scene entries: the kernel without those paths (a smaller instruction footprint)
         IK_DISPATCH(G, lm_persistent_core, {
             rc = prepare_kernel(kfn, smem);
             if (rc) return rc;

@@ -365,6 +365,7 @@ struct Tabs {
     IK_TAB(PoseEntry, pose, o_pose)
     IK_TAB(CollEntry, coll, o_coll)
     IK_TAB(JointRefEntry, jref, o_jref)
+    IK_TAB(SceneEntry, scene, o_scene)
     IK_TAB(float, limw, o_limw)
     IK_TAB(float, mask, o_mask)
     IK_TAB(uint16_t, ab, o_ab)
@@ -572,6 +573,148 @@ __device__ __forceinline__ float collision_column(const Tabs& t, const float* S,
 }
 
 // ---------------------------------------------------------------------------
+// Scene collision over primitive geometry (scene_collision_task.py:276-650).
+// ---------------------------------------------------------------------------
+// d(point)/d(tangent column c) of a point p fixed to `link`
+// (scene_distance_task.py:44-70): base columns Ad(T_world_base) e_c, joint
+// columns the contributing joints' world twists v + om x p.
+__device__ __forceinline__ V3 point_column(const Tabs& t, const float* S, const float* base, int c, int link, V3 p) {
+    const int boff = t.h->base_off;
+    if (c < boff) {
+        const Pose B = pose_load(base);
+        const V3 e{c % 3 == 0 ? 1.f : 0.f, c % 3 == 1 ? 1.f : 0.f, c % 3 == 2 ? 1.f : 0.f};
+        const V3 Re = qrot(B.w, B.i, B.j, B.k, e);
+        if (c < 3) return Re;
+        return cross(Re, V3{p.x - B.x, p.y - B.y, p.z - B.z});
+    }
+    const int a = c - boff;
+    const unsigned long long anc = t.lanc()[link];
+    V3 col{0.f, 0.f, 0.f};
+    for (int idx = t.colstart()[a]; idx < t.colstart()[a + 1]; ++idx) {
+        const int j = t.coljoint()[idx];
+        if (!((anc >> j) & 1ull)) continue;
+        const float* s = S + 8 * j;
+        const V3 v{s[0], s[1], s[2]}, om{s[3], s[4], s[5]};
+        const V3 cj = v + cross(om, p);
+        const float m = t.colmul()[idx];
+        col = V3{col.x + m * cj.x, col.y + m * cj.y, col.z + m * cj.z};
+    }
+    return col;
+}
+
+// Nearest primitive of scene `sid` to world point p: the first of strictly
+// least signed distance in query order, its world normal
+// (geom/sdf_kernels.py:223-344); an empty scene gives 1e6 and a zero normal
+// (geom/geoms.py:29).
+struct SdfHit {
+    float dist;
+    V3 n;
+};
+__device__ __forceinline__ SdfHit scene_query(const Tabs& t, const SceneEntry& se, int sid, V3 p) {
+    const float4* el = t.at<float4>(se.o_elem);
+    const int* off = t.at<int>(se.o_off);
+    SdfHit hit{1.0e6f, V3{0.f, 0.f, 0.f}};
+    for (int e = off[sid]; e < off[sid + 1]; ++e) {
+        const float4 r0 = el[5 * e], r1 = el[5 * e + 1], r2 = el[5 * e + 2], prm = el[5 * e + 3], ts = el[5 * e + 4];
+        const float s = ts.y;
+        V3 ql{fmaf(r0.x, p.x, fmaf(r0.y, p.y, fmaf(r0.z, p.z, r0.w))),
+              fmaf(r1.x, p.x, fmaf(r1.y, p.y, fmaf(r1.z, p.z, r1.w))),
+              fmaf(r2.x, p.x, fmaf(r2.y, p.y, fmaf(r2.z, p.z, r2.w)))};
+        if (s != 1.f) ql = V3{ql.x / s, ql.y / s, ql.z / s};
+        float un;
+        V3 nl{0.f, 0.f, 1.f};
+        const int type = (int)ts.x;
+        if (type == IK_GEOM_BOX) {
+            const V3 qv{fabsf(ql.x) - prm.x, fabsf(ql.y) - prm.y, fabsf(ql.z) - prm.z};
+            const float qmax = fmaxf(fmaxf(qv.x, qv.y), qv.z);
+            const V3 qp{fmaxf(qv.x, 0.f), fmaxf(qv.y, 0.f), fmaxf(qv.z, 0.f)};
+            un = norm3(qp) + fminf(qmax, 0.f);
+            if (qmax < 0.f) {  // inside: the nearest face
+                if (qv.x >= qv.y && qv.x >= qv.z)
+                    nl = V3{ql.x < 0.f ? -1.f : 1.f, 0.f, 0.f};
+                else if (qv.y >= qv.z)
+                    nl = V3{0.f, ql.y < 0.f ? -1.f : 1.f, 0.f};
+                else
+                    nl = V3{0.f, 0.f, ql.z < 0.f ? -1.f : 1.f};
+            } else {
+                const V3 d{ql.x - fminf(fmaxf(ql.x, -prm.x), prm.x), ql.y - fminf(fmaxf(ql.y, -prm.y), prm.y),
+                           ql.z - fminf(fmaxf(ql.z, -prm.z), prm.z)};
+                const float dl = norm3(d);
+                if (dl > 1.0e-10f) nl = V3{d.x / dl, d.y / dl, d.z / dl};
+            }
+        } else if (type == IK_GEOM_SPHERE) {
+            const float ql2 = norm3(ql);
+            un = ql2 - prm.x;
+            nl = ql2 > 1.0e-10f ? V3{ql.x / ql2, ql.y / ql2, ql.z / ql2} : V3{1.f, 0.f, 0.f};
+        } else if (type == IK_GEOM_PLANE) {
+            un = ql.z;
+        } else {  // capsule along local z
+            const float tz = fminf(fmaxf(ql.z, -prm.y), prm.y);
+            const V3 d{ql.x, ql.y, ql.z - tz};
+            const float dl = norm3(d);
+            un = dl - prm.x;
+            nl = dl > 1.0e-10f ? V3{d.x / dl, d.y / dl, d.z / dl} : V3{1.f, 0.f, 0.f};
+        }
+        const float dist = un * s;
+        if (dist < hit.dist) {
+            hit.dist = dist;
+            // world normal R n_local: the rows of R^T are the columns of R
+            hit.n = V3{r0.x * nl.x + r1.x * nl.y + r2.x * nl.z, r0.y * nl.x + r1.y * nl.y + r2.y * nl.z,
+                       r0.z * nl.x + r1.z * nl.y + r2.z * nl.z};
+        }
+    }
+    return hit;
+}
+
+// Penalty of signed distance sd and its derivative (terms/sphere_collision_kernels.py:17-41).
+__device__ __forceinline__ float2 scene_penalty(float sd, float margin, int mode) {
+    if (mode == IK_PENALTY_SURFACE_DISTANCE) return make_float2(fabsf(sd), sd > 0.f ? 1.f : (sd < 0.f ? -1.f : 0.f));
+    if (mode == IK_PENALTY_PLAIN) return sd < margin ? make_float2(margin - sd, -1.f) : make_float2(0.f, 0.f);
+    if (sd < 0.f) return make_float2(0.5f * margin - sd, -1.f);
+    if (sd <= margin) {
+        const float diff = sd - margin;
+        const float inv = 1.f / (margin + 1e-6f);
+        return make_float2(0.5f * inv * diff * diff, inv * diff);
+    }
+    return make_float2(0.f, 0.f);
+}
+
+// Row k of a scene term at the current sphere centres: the weighted residual,
+// whether its Jacobian row is non-zero, and the factor `scale` with which
+// row = scale * n . d(centre)/d(tangent) (scene_collision_task.py:34-82).
+struct SceneRow {
+    float r, scale;
+    V3 n, p;
+    int link;
+    bool act;
+};
+__device__ __forceinline__ SceneRow scene_row(const Tabs& t, const Ws& w, const SceneEntry& se, int sid, int k) {
+    const int s = t.at<int>(se.o_q)[k];
+    const float wk = t.at<float>(se.o_w)[k];
+    const float4 c = *reinterpret_cast<const float4*>(w.sph() + 4 * s);
+    SceneRow o;
+    o.p = V3{c.x, c.y, c.z};
+    o.link = t.sphlink()[s];
+    const SdfHit hit = scene_query(t, se, sid, o.p);
+    o.n = hit.n;
+    const float sd = hit.dist - c.w;
+    const float2 pp = scene_penalty(sd, se.margin, se.penalty);
+    float res = pp.x, sc = pp.y;
+    if (se.use_sqrt) {
+        if (pp.x > 0.f) sc *= 0.5f / sqrtf(pp.x + se.eps);
+        res = sqrtf(pp.x + se.eps);
+    }
+    o.r = wk * res;
+    o.scale = wk * sc;
+    o.act = se.penalty == IK_PENALTY_SURFACE_DISTANCE || sd <= se.margin;
+    return o;
+}
+
+__device__ __forceinline__ int scene_of(const Ws& w, const SceneEntry& se) {
+    return reinterpret_cast<const int*>(w.misc())[se.misc];
+}
+
+// ---------------------------------------------------------------------------
 // Broad phase of a collision term: link pairs whose bounding spheres come
 // within the margin (+ `inflate`), in link-pair order, into `list` (at most
 // `cap`).  With inflate = 0 and the exact distance this is the reference's
@@ -694,7 +837,7 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
     o.Tj = group_fk<G>(g, t, w, q, base);
     o.S = (o.Tj == w.T0()) ? w.T1() : w.T0();
     float* Tj = o.Tj;
-    const bool need_sph = h->ncoll > 0;
+    const bool need_sph = h->ncoll > 0 || (F && h->nscene > 0);
     if (need_sph) {
         for (int s = g.lane; s < h->ns; s += G) {
             const Pose P = link_pose(t, Tj, base, t.sphlink()[s]);
@@ -833,6 +976,15 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
             }
             reinterpret_cast<int*>(w.misc())[8 + ci] = nsl;
             o.nslots += nsl;
+        }
+    }
+    // scene collision, scene_collision_task.py:550-592
+    for (int k = 0; F && k < h->nscene; ++k) {
+        const SceneEntry& se = t.scene()[k];
+        const int sid = scene_of(w, se);
+        for (int i = g.lane; i < se.nq; i += G) {
+            const float r = scene_row(t, w, se, sid, i).r;
+            kadd(ks, kc, r * r);
         }
     }
     o.cost = 0.5f * group_ksum<G>(g, ks, kc);
@@ -1175,6 +1327,35 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
                     group_accumulate_chunk<G>(g, t, w, filled);
                 }
             }
+        }
+    }
+    // scene-collision rows with a non-zero Jacobian, compacted into chunks
+    for (int k = 0; F && k < h->nscene; ++k) {
+        const SceneEntry& se = t.scene()[k];
+        const int sid = scene_of(w, se);
+        const int D = h->D, Dp = h->Dp;
+        int filled = 0;
+        for (int b0 = 0; b0 < se.nq; b0 += G) {
+            const int i = b0 + g.lane;
+            SceneRow sr;
+            sr.act = false;
+            if (i < se.nq) sr = scene_row(t, w, se, sid, i);
+            const unsigned bal = g.ballot(sr.act);
+            if (sr.act) {
+                float* J = w.Jc() + (filled + __popc(bal & g.lt_mask())) * Dp;
+                for (int c = 0; c < D; ++c) J[c] = sr.scale * dot(sr.n, point_column(t, S, base, c, sr.link, sr.p));
+                J[D] = sr.r;
+            }
+            filled += __popc(bal);
+            if (filled > kChunkRows - G) {
+                g.sync();
+                group_accumulate_chunk<G>(g, t, w, filled);
+                filled = 0;
+            }
+        }
+        if (filled > 0) {
+            g.sync();
+            group_accumulate_chunk<G>(g, t, w, filled);
         }
     }
     // finalise: fold compensation, joint-limit diagonal, active-DOF mask

@@ -46,6 +46,9 @@ struct TermHost {
     std::vector<int> frame_links;
     std::vector<float> weights;
     std::vector<float> vlim;  // velocity-limit terms: [na]
+    std::vector<int> qsph;      // scene collision: queried sphere indices
+    std::vector<float> selem;   // scene collision: primitive records (5 float4 each), sorted by scene
+    std::vector<int> soff;      // scene collision: CSR offsets per scene
     std::vector<int> lp, lpoff, sp;
     int row = 0, rows = 0;
 };

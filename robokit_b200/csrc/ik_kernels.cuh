@@ -194,6 +194,10 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 const JointRefEntry& jr = t.jref()[je];
                 for (int a = g.lane; a < h->na; a += G) ro[jr.out_row + a] = jref_row(t, w, jr, w.q[a], a).r;
             }
+            for (int k = 0; k < h->nscene; ++k) {
+                const SceneEntry& se = t.scene()[k];
+                for (int i = g.lane; i < se.nq; i += G) ro[se.out_row + i] = scene_row(t, w, se, scene_of(w, se), i).r;
+            }
         }
         float* S = ev.S;
         for (int j = g.lane; j < h->nj; j += G) {
@@ -236,6 +240,15 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 const JointRefEntry& jr = t.jref()[je];
                 for (int a = g.lane; a < h->na; a += G)
                     Jo[(size_t)(jr.out_row + a) * D + boff + a] = jref_row(t, w, jr, w.q[a], a).js;
+            }
+            for (int k = 0; k < h->nscene; ++k) {
+                const SceneEntry& se = t.scene()[k];
+                for (int i = g.lane; i < se.nq; i += G) {
+                    const SceneRow sr = scene_row(t, w, se, scene_of(w, se), i);
+                    for (int c = 0; c < D; ++c)
+                        Jo[(size_t)(se.out_row + i) * D + c] =
+                            sr.act ? sr.scale * dot(sr.n, point_column(t, S, b, c, sr.link, sr.p)) : 0.f;
+                }
             }
         }
         for (int ci = 0; ci < h->ncoll; ++ci) {

@@ -45,6 +45,18 @@ __device__ __forceinline__ void load_point(const Group<G>& g, const Tabs& t, Ws&
 template <int G>
 __device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
     const TabHeader* h = t.h;
+    // the problem's scene per scene term (scene_collision_task.py:486-500: row b / (batch / rows)),
+    // clamped to the scenes that exist
+    for (int k = g.lane; k < h->nscene; k += G) {
+        const SceneEntry& se = t.scene()[k];
+        int sid = 0;
+        if (se.scene_rows > 0) {
+            int rep = batch / se.scene_rows;
+            if (rep < 1) rep = 1;
+            sid = se.scene_idx[min(p / rep, se.scene_rows - 1)];
+        }
+        reinterpret_cast<int*>(w.misc())[se.misc] = min(max(sid, 0), se.nscenes - 1);
+    }
     for (int je = 0; je < h->njref; ++je) {
         const JointRefEntry& jr = t.jref()[je];
         const int rows = jr.target_rows > 0 ? jr.target_rows : batch;

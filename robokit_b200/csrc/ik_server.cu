@@ -569,9 +569,11 @@ int ik_server_add_type(IkServer* S, IkRobot* robot, int32_t floating_base, const
     T->slots = slots;
     T->params = *params;
     for (int i = 0; i < num_terms; ++i)
-        if (descs[i].kind == IK_TERM_JOINT_REF || descs[i].kind == IK_TERM_VELOCITY_LIMIT) {
+        if (descs[i].kind == IK_TERM_JOINT_REF || descs[i].kind == IK_TERM_VELOCITY_LIMIT ||
+            descs[i].kind == IK_TERM_SCENE_COLLISION) {
             delete T;
-            return fail(IK_E_UNSUPPORTED, "term %d: joint-reference terms are not served (no per-request references)", i);
+            return fail(IK_E_UNSUPPORTED, "term %d: joint-reference and scene terms are not served (no per-request "
+                        "references or scenes)", i);
         } else if (descs[i].kind == IK_TERM_POSITION || descs[i].kind == IK_TERM_ROTATION || descs[i].kind == IK_TERM_FRAME) {
             if (descs[i].num_frames < 1) {
                 delete T;

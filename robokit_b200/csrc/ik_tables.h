@@ -82,6 +82,30 @@ struct JointRefEntry {
 };
 static_assert(sizeof(JointRefEntry) == 32, "JointRefEntry layout");
 
+// One SceneCollisionTask over primitive geometry (scene_collision_task.py:276-650):
+// robot sphere centres against the primitives of the problem's scene.
+// Primitive records: 5 float4 each — the three rows of the inverse pose
+// [R^T | -R^T t], the parameters, and (type, scale, 0, 0) — sorted by scene
+// (stable, so a point meets them in query order); CSR offsets per scene.
+struct SceneEntry {
+    int32_t out_row;      // first row in the reference layout
+    int32_t nq;           // robot spheres queried (one row each)
+    int32_t o_q;          // int32 [nq] sphere indices
+    int32_t o_w;          // float [nq] weights
+    int32_t o_elem;       // float4 [nelem * 5] primitive records
+    int32_t o_off;        // int32 [nscenes + 1] CSR offsets into the records
+    int32_t nscenes;
+    int32_t penalty;      // IK_PENALTY_*
+    int32_t use_sqrt;     // residual sqrt(penalty + eps)
+    float margin;         // activation distance
+    float eps;
+    int32_t scene_rows;   // rows of scene_idx (0: scene 0 for every problem)
+    const int32_t* scene_idx;  // device [scene_rows]
+    int32_t misc;         // workspace misc slot holding the problem's scene index
+    int32_t pad;
+};
+static_assert(sizeof(SceneEntry) == 64, "SceneEntry layout");
+
 struct TabHeader {
     int32_t bytes;        // blob size, multiple of 16
     int32_t nj, nl, na, ns;
@@ -117,7 +141,8 @@ struct TabHeader {
     int32_t thread_ok;    // 1 when the lane-per-problem kernels can run this problem
     int32_t t_floats;
     int32_t t_Tj, t_S, t_sph, t_tgt, t_Hs, t_Hc, t_q, t_qp, t_base, t_basep;
-    int32_t pad[2];
+    int32_t nscene;       // scene-collision terms (at most IK_SCENE_MAX_TERMS)
+    int32_t o_scene;      // blob offset of the SceneEntry table
 };
 
 }  // namespace b200ik

@@ -6,7 +6,8 @@ PositionTask (terms/dense/position_task.py:18-272), RotationTask
 (terms/dense/position_limit.py:185-573), the joint blocks of SmoothnessTask
 (terms/dense/smoothness_task.py:22-460) and ConfigurationTask
 (terms/dense/configuration_task.py:25-478), VelocityLimitTask
-(terms/dense/velocity_limit_task.py:14-232), and SelfCollisionTask with sphere
+(terms/dense/velocity_limit_task.py:14-232), SceneCollisionTask over primitive
+geometry (terms/dense/scene_collision_task.py:276-650), and SelfCollisionTask with sphere
 geometry (terms/dense/self_collision_task.py:593-1152).  Constructor
 signatures, defaults, residual_dim and set_weight / set_target follow the
 reference; the arithmetic runs in libb200ik.so.
@@ -511,6 +512,142 @@ class VelocityLimitTask(_JointRefTask):
             return
         self._prev_q = new.clone() if isinstance(new, N.DeviceArray) else new
         self._touch()
+
+
+_PENALTIES = {"smooth": N.IK_PENALTY_SMOOTH, "plain": N.IK_PENALTY_PLAIN,
+              "surface_distance": N.IK_PENALTY_SURFACE_DISTANCE}
+
+
+class SceneCollisionTask(ResidualTask):
+    """Penalise robot collision spheres that approach scene geometry (scene_collision_task.py:276-650).
+
+    One row per queried sphere: w * penalty(sdf(centre) - radius) with the
+    reference's "smooth" (default), "plain" or "surface_distance" penalty and
+    the "abs" or "sqrt_abs" residual.  The scene holds primitives (boxes,
+    spheres, planes, capsules; robokit_b200.geom); `scene_indices` picks each
+    problem's scene (row b // (batch // rows)).  The link bounding-sphere
+    filter only skips queries whose rows are zero anyway, so it is accepted and
+    changes nothing here."""
+
+    def __init__(self, robot: Any = None, scene: Any = None, geometry: Any = None, scene_indices: Any = None,
+                 use_link_bounding_sphere_filter: bool = False, weight: Union[float, Sequence[float]] = 1.0,
+                 margin: Optional[float] = 0.02, sphere_indices: Optional[Sequence[int]] = None,
+                 residual_mode: Literal["abs", "sqrt_abs"] = "abs", residual_eps: float = 1e-6,
+                 penalty: Literal["smooth", "plain", "surface_distance"] = "smooth",
+                 skip_trajectory_endpoints: bool = True, movable_only: bool = False, name: str = ""):
+        if penalty not in _PENALTIES:
+            raise ValueError(f"Unsupported penalty: {penalty}")
+        if residual_mode not in ("abs", "sqrt_abs"):
+            raise ValueError(f"Unsupported residual_mode: {residual_mode}")
+        if use_link_bounding_sphere_filter and penalty == "surface_distance":
+            raise NotImplementedError("the link filter with the surface-distance penalty is not supported")
+        self.name = name
+        self.robot = robot
+        self.scene = scene
+        self.geometry = geometry
+        self.scene_indices = scene_indices
+        self.use_link_bounding_sphere_filter = use_link_bounding_sphere_filter
+        self.weight = weight
+        self.margin = 0.0 if margin is None else float(margin)
+        self.sphere_indices = sphere_indices
+        self.residual_mode = residual_mode
+        self.residual_eps = residual_eps
+        self.penalty = penalty
+        self.skip_trajectory_endpoints = skip_trajectory_endpoints
+        self.movable_only = movable_only
+        self._own_version = 0
+        self._scene_idx_dev: Optional[N.DeviceArray] = None
+        if robot is None or isinstance(scene, Context) or isinstance(scene_indices, Context):
+            return  # configuration-time stub
+        self.set_robot(robot)
+        if scene_indices is not None:
+            self.set_scene_indices(scene_indices)
+
+    # -- configuration ----------------------------------------------------------------
+    @property
+    def _version(self) -> Any:
+        rev = self.scene.revision if self.scene is not None and not isinstance(self.scene, Context) else 0
+        return (self._own_version, rev)
+
+    def _touch(self) -> None:
+        self._own_version += 1
+
+    @property
+    def active(self) -> bool:
+        """Nonzero weight and a scene with geometry, or a helper's scene to come."""
+        if self.scene is None:
+            return False
+        if not isinstance(self.scene, Context) and self.scene.num_elements == 0:
+            return False
+        return bool(np.any(np.asarray(self.weight, np.float32)))
+
+    def set_robot(self, robot: Any) -> None:
+        self.robot = robot
+        spec = robot.spec
+        ns = len(spec.collision_sphere_radii)
+        if ns == 0:
+            raise RuntimeError("Robot has no collision spheres. Load with load_collision_spheres=True.")
+        if self.sphere_indices is None and self.movable_only:
+            self.sphere_indices = np.flatnonzero(np.asarray(spec.collision_spheres_link_indices) > 0)
+        idx = np.arange(ns, dtype=np.int32) if self.sphere_indices is None else np.asarray(self.sphere_indices,
+                                                                                           np.int32)
+        if idx.ndim != 1:
+            raise ValueError("sphere_indices must be 1D.")
+        if np.any(idx < 0) or np.any(idx >= ns):
+            raise ValueError("sphere_indices contains out-of-range indices.")
+        self._sphere_idx = idx
+        w = np.ones(idx.shape[0], np.float32)
+        if isinstance(self.weight, (int, float)):
+            w[:] = float(self.weight)
+        else:
+            wa = np.asarray(self.weight, np.float32)
+            if wa.shape != (idx.shape[0],):
+                raise ValueError(f"Expected weight shape ({idx.shape[0]},), got {wa.shape}.")
+            w[:] = wa
+        self._weights = w
+        self._touch()
+
+    def set_weight(self, weight: Union[float, Sequence[float]]) -> None:
+        self.weight = weight
+        if self.robot is not None:
+            self.set_robot(self.robot)
+
+    def set_scene_indices(self, scene_indices: Any) -> None:
+        """The scene of each problem row, int32 (scene_collision_task.py:412-437); read in place when on the device."""
+        if isinstance(scene_indices, N.DeviceArray) or hasattr(scene_indices, "__cuda_array_interface__"):
+            d = N.as_device(scene_indices, np.int32)
+        else:
+            d = N.DeviceArray.from_numpy(np.ascontiguousarray(scene_indices, np.int32).reshape(-1))
+        if d.ndim != 1 or d.shape[0] < 1:
+            raise ValueError("scene_indices must be a non-empty 1D int32 array.")
+        self.scene_indices = d
+        self._scene_idx_dev = d
+        self._touch()
+
+    @property
+    def residual_dim(self) -> int:
+        return int(self._sphere_idx.shape[0])
+
+    # -- lowering -----------------------------------------------------------------------
+    def _desc(self, var: Any, scene_idx: Any) -> Dict[str, Any]:
+        if self.robot is None or self.scene is None or isinstance(self.scene, Context):
+            raise ValueError("SceneCollisionTask needs a robot and a scene (build it through a helper or pass both)")
+        if var.spec.num_links != self.robot.spec.num_links:
+            raise ValueError("term built for another robot")
+        if scene_idx is not None and var.batch_size % scene_idx.shape[0]:
+            raise ValueError("scene_indices must have shape (batch_size,) or divide it (one scene per candidate "
+                             "group).")
+        return dict(kind=N.IK_TERM_SCENE_COLLISION, weights=self._weights, query_spheres=self._sphere_idx,
+                    geoms=self.scene.records(self.geometry), num_scenes=self.scene.num_scenes,
+                    penalty=_PENALTIES[self.penalty], residual_sqrt=self.residual_mode == "sqrt_abs",
+                    residual_eps=float(self.residual_eps), margin=self.margin, scene_indices=scene_idx)
+
+    def native_desc(self, var: Any) -> Dict[str, Any]:
+        return self._desc(var, self._scene_idx_dev)
+
+    def host_desc(self, var: Any) -> Dict[str, Any]:
+        si = None if self._scene_idx_dev is None else self._scene_idx_dev.numpy()
+        return self._desc(var, si)
 
 
 class SelfCollisionTask(ResidualTask):

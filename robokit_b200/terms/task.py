@@ -149,6 +149,22 @@ def lower_terms(robot: Any, terms: List[ResidualTask], capacity: int, floating: 
         descs[i].sphere_pairs = arr(d.get("sphere_pairs"), np.int32)
         descs[i].dt = d.get("dt", 0.0)
         descs[i].velocity_limits = arr(d.get("velocity_limits"), np.float32)
+        qs = d.get("query_spheres")
+        if qs is not None:
+            descs[i].num_query_spheres = len(qs)
+            descs[i].query_spheres = arr(qs, np.int32)
+            gm = np.asarray(d.get("geoms"), np.float32)
+            descs[i].num_geoms = gm.size // N.IK_GEOM_FLOATS
+            descs[i].geoms = arr(gm, np.float32)
+            descs[i].num_scenes = d["num_scenes"]
+            descs[i].penalty = d["penalty"]
+            descs[i].residual_sqrt = int(bool(d.get("residual_sqrt", 0)))
+            descs[i].residual_eps = d.get("residual_eps", 0.0)
+            si = d.get("scene_indices")
+            if si is not None:
+                keep.append(si)
+                descs[i].d_scene_indices = si.ptr
+                descs[i].scene_rows = si.shape[0]
     return descs
 
 

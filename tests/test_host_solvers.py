@@ -149,3 +149,54 @@ def test_velocity_limit_term_host_side(panda_spec):
     s = RobotSpec.from_records("r", ["l0", "l1", "l2", "l3"], recs)
     np.testing.assert_array_equal(s.joint_velocity_limits, [3.0, 10.0, 0.0])
     np.testing.assert_array_equal(s.actuated_joint_velocity_limits, [3.0, 10.0])
+
+
+def test_scene_geometry_and_term_host_side(panda_collision_spec):
+    """Primitive records in query order, CSR validation, and the scene term's lowering and argument checks."""
+    from robokit_b200.geom import BoxGeom, CapsuleGeom, PlaneGeom, Scene, SphereGeom
+    from robokit_b200.terms.dense import SceneCollisionTask
+
+    s = Scene(num_scenes=2)
+    box = BoxGeom([[0.1, 0.2, 0.3], [1, 1, 1]], [0, 1, 2], poses=np.eye(4)[None].repeat(2, 0))
+    s.add(box).add(SphereGeom([0.5], [0, 0, 1])).add(PlaneGeom([0, 1, 1])).add(CapsuleGeom([0.1], [0.4], [0, 1, 1]))
+    rec = s.records()
+    assert rec.shape == (5, N.IK_GEOM_FLOATS)
+    np.testing.assert_array_equal(rec[:, 0], [N.IK_GEOM_BOX, N.IK_GEOM_BOX, N.IK_GEOM_SPHERE, N.IK_GEOM_PLANE,
+                                              N.IK_GEOM_CAPSULE])
+    np.testing.assert_array_equal(rec[:, 1], [0, 1, 1, 0, 0])
+    np.testing.assert_allclose(rec[0, 4:8], [0.1, 0.2, 0.3, 0])
+    np.testing.assert_allclose(rec[0, 8:15], [0, 0, 0, 1, 0, 0, 0])
+    np.testing.assert_allclose(rec[4, 4:6], [0.1, 0.4])
+    rev = s.revision
+    box.update(poses=[[0, 0, 1, 1, 0, 0, 0], [0, 0, 2, 1, 0, 0, 0]])
+    assert s.revision > rev and s.records()[1, 10] == 2.0
+    with pytest.raises(ValueError):
+        BoxGeom([[1, 1, 1]], [0, 2])
+    with pytest.raises(ValueError):
+        s.add(SphereGeom([1.0], [0, 1]))  # one scene in a two-scene scene
+    with pytest.raises(ValueError):
+        Scene(1, device="cpu")
+
+    class _Robot:
+        spec = panda_collision_spec
+
+    class _V:
+        spec, batch_size, has_floating_base = panda_collision_spec, 8, False
+
+    ns = len(panda_collision_spec.collision_sphere_radii)
+    t = SceneCollisionTask(_Robot(), s, weight=2.0, margin=0.05, penalty="plain", residual_mode="sqrt_abs")
+    d = t.host_desc(_V)
+    assert d["kind"] == N.IK_TERM_SCENE_COLLISION and t.residual_dim == ns and d["num_scenes"] == 2
+    assert d["penalty"] == N.IK_PENALTY_PLAIN and d["residual_sqrt"] and np.all(d["weights"] == 2.0)
+    mov = SceneCollisionTask(_Robot(), s, movable_only=True)
+    assert mov.residual_dim == int(np.sum(panda_collision_spec.collision_spheres_link_indices > 0))
+    v0 = t._version
+    s.add(PlaneGeom([0, 1, 1]))
+    assert t._version != v0  # a changed scene rebuilds the terms that read it
+    with pytest.raises(ValueError, match="Unsupported penalty"):
+        SceneCollisionTask(_Robot(), s, penalty="hard")
+    with pytest.raises(ValueError, match="out-of-range"):
+        SceneCollisionTask(_Robot(), s, sphere_indices=[ns])
+    with pytest.raises(ValueError, match="weight shape"):
+        SceneCollisionTask(_Robot(), s, weight=[1.0, 2.0])
+    assert not SceneCollisionTask(_Robot(), Scene(1)).active

@@ -272,3 +272,78 @@ def test_oracle_velocity_limit_term(panda_spec):
     expect = np.zeros((B, na, na))
     expect[:, np.arange(na), np.arange(na)] = np.where(act, w * np.sign(qd) / np.float32(dt), 0.0)
     np.testing.assert_allclose(J, expect, rtol=1e-12, atol=0)
+
+
+def _scene_records(rows):
+    """[n, 16] primitive records: (type, scene, scale, params, pose vec7)."""
+    out = np.zeros((len(rows), 16), np.float32)
+    for i, (typ, scene, scale, prm, pose) in enumerate(rows):
+        out[i, 0], out[i, 1], out[i, 2] = typ, scene, scale
+        out[i, 4:4 + len(prm)] = prm
+        p = np.asarray(pose, np.float64)
+        p[3:] /= np.linalg.norm(p[3:])
+        out[i, 8:15] = p
+    return out
+
+
+@pytest.mark.parametrize("prim", ["box", "sphere", "plane", "capsule"])
+@pytest.mark.parametrize("penalty", [0, 1, 2])
+def test_oracle_scene_term_matches_finite_differences(panda_collision_spec, prim, penalty):
+    """Scene-collision rows of the oracle: the Jacobian agrees with central differences of the residual for each
+    primitive type and penalty, with and without a floating base; rows beyond the margin are zero."""
+    spec = panda_collision_spec
+    rob = oracle.Robot.from_spec(spec)
+    rng = np.random.default_rng(4)
+    rot = [0.9, 0.2, -0.3, 0.25]
+    # placed against the arm at this configuration (sphere centres span x 0-0.65 m, z 0.08-0.9 m)
+    geo = {"box": (0, [0.12, 0.08, 0.08], [0.4, 0.15, 0.55] + rot),
+           "sphere": (1, [0.1], [0.35, 0.15, 0.55] + rot),
+           "plane": (2, [], [0.0, 0.0, 0.6] + [0.99, 0.05, -0.05, 0.0]),
+           "capsule": (3, [0.05, 0.12], [0.45, 0.15, 0.58] + rot)}[prim]
+    rec = _scene_records([(geo[0], 0, 1.3, geo[1], geo[2])])
+    ns = len(spec.collision_sphere_radii)
+    term = dict(kind=8, weights=np.linspace(0.5, 2.0, ns), query_spheres=np.arange(ns), geoms=rec, num_scenes=1,
+                penalty=penalty, margin=0.15, residual_sqrt=0, residual_eps=1e-6)
+    terms = oracle.Terms([term])
+    assert oracle.residual_dim(rob, terms) == ns
+    q = (spec.midrange_q + rng.normal(0, 0.3, spec.num_actuated_joints)).astype(np.float64)
+    for base in (None, np.array([[0.05, -0.02, 0.03, 0.98, 0.05, -0.1, 0.1]])):
+        if base is not None:
+            base[:, 3:] /= np.linalg.norm(base[:, 3:])
+            base = base.astype(np.float32)
+        boff = 0 if base is None else 6
+        r, J = oracle.residual_jacobian(rob, terms, q[None].astype(np.float32), base)
+        if penalty != 2:
+            assert (r[0] > 0).any() and (r[0] == 0).any()
+        eps = 1e-4
+        for a in range(spec.num_actuated_joints):
+            qp, qm = q.copy(), q.copy()
+            qp[a] += eps
+            qm[a] -= eps
+            rp, _ = oracle.residual_jacobian(rob, terms, qp[None], base)
+            rm, _ = oracle.residual_jacobian(rob, terms, qm[None], base)
+            fd = (rp[0] - rm[0]) / (2 * eps)
+            # the hinge's kink and the box's face switches are the only places where the two may differ
+            smooth = (np.abs(r[0]) > 1e-3) | (J[0][:, boff + a] == 0)
+            np.testing.assert_allclose(J[0][smooth, boff + a], fd[smooth], atol=2e-3, rtol=1e-3)
+
+
+def test_oracle_scene_selection_and_query_order(panda_collision_spec):
+    """Each problem reads its scene (row b // (B // rows)); a point keeps the first primitive of least distance;
+    an empty scene leaves every sphere at 1e6."""
+    spec = panda_collision_spec
+    rob = oracle.Robot.from_spec(spec)
+    ns = len(spec.collision_sphere_radii)
+    rec = _scene_records([(2, 0, 1.0, [], [0, 0, 0.2, 1, 0, 0, 0]),     # scene 0: plane z = 0.2
+                          (2, 1, 1.0, [], [0, 0, 0.6, 1, 0, 0, 0]),     # scene 1: plane z = 0.6 ...
+                          (2, 1, 1.0, [], [0, 0, 0.6, 1, 0, 0, 0])])    # ... twice (ties keep the first)
+    q = np.tile(spec.midrange_q, (4, 1)).astype(np.float32)
+    term = dict(kind=8, weights=np.ones(ns), query_spheres=np.arange(ns), geoms=rec, num_scenes=3, penalty=2,
+                margin=0.02, residual_sqrt=0, residual_eps=1e-6, scene_indices=np.array([1, 2], np.int32))
+    r, _ = oracle.residual_jacobian(rob, oracle.Terms([term]), q)
+    c = oracle.fk(rob, q[:1])["spheres"][0]
+    expect = np.abs(c[:, 2] - 0.6 - spec.collision_sphere_radii)  # problems 0, 1: scene 1
+    np.testing.assert_allclose(r[0], expect, rtol=1e-9, atol=1e-7)  # radii are stored as float32
+    np.testing.assert_allclose(r[1], expect, rtol=1e-9, atol=1e-7)
+    np.testing.assert_allclose(r[2:], np.broadcast_to(1e6 - spec.collision_sphere_radii.astype(np.float32), (2, ns)),
+                               rtol=1e-6)
