@@ -24,6 +24,16 @@ class IKContext(Context):
     """The previous solution (batch,), from solve(prev_state=...); zeros until the first one."""
     REST_Q = 4
     """Rest configurations (batch, dofs): the zero configuration until solve(rest_state=...)."""
+    REST_BASE = 5
+    """Rest base poses; a fixed base has none (templates on it are not supported here)."""
+    NUM_SOLUTIONS = 6
+    """Solutions each target returns."""
+    OPTIMIZATION_TERMS = 7
+    """The built optimization terms (score terms are not supported here)."""
+    SCENE = 8
+    """The collision scene, from IKSolver(scene=...); None without one."""
+    SCENE_INDICES = 9
+    """Each target's scene (batch,): zeros until solve(scene_indices=...)."""
 
 
 def _default_solver() -> PopulationSolverConfig:

@@ -11,9 +11,10 @@ Everything between the host call and the result runs on the GPU: the spread
 select launch between stages.  The term templates of the config (PositionTask,
 RotationTask, FrameTask with IKContext placeholders, PositionLimit,
 SelfCollisionTask, SmoothnessTask and VelocityLimitTask on
-IKContext.PREVIOUS_STATE, ConfigurationTask on IKContext.REST_Q) become concrete terms that read the solver's target,
-previous-state and rest buffers in place with the reference's broadcast rule
-(candidate c of target b reads row b).  With a previous state, each target keeps
+IKContext.PREVIOUS_STATE, ConfigurationTask on IKContext.REST_Q,
+SceneCollisionTask on IKContext.SCENE / SCENE_INDICES) become concrete terms
+that read the solver's target, previous-state, rest and scene-index buffers in
+place with the reference's broadcast rule (candidate c of target b reads row b).  With a previous state, each target keeps
 it where it scores no worse than the solve's result (helpers/ik/ik.py:257-289).
 """
 
@@ -30,8 +31,8 @@ from ...opt.lm_optimizer import LMOptimizer, LMOptimizerConfig
 from ...opt.sampler import RobertsSampler
 from ...opt.var_values import VarKey, VarValues
 from ...robo.robot_state import RobotState
-from ...terms.dense import (ConfigurationTask, FrameTask, PositionLimit, PositionTask, RotationTask, SelfCollisionTask,
-                            SmoothnessTask, VelocityLimitTask, _PoseTask)
+from ...terms.dense import (ConfigurationTask, FrameTask, PositionLimit, PositionTask, RotationTask,
+                            SceneCollisionTask, SelfCollisionTask, SmoothnessTask, VelocityLimitTask, _PoseTask)
 from ...terms.task import Context
 from .config import IKContext, IKSolverConfig
 
@@ -48,8 +49,7 @@ class IKMetrics:
 class IKSolver:
     def __init__(self, config: IKSolverConfig, robot: Any, target_links: Union[str, int, Sequence[Union[str, int]]],
                  device: Any = "cuda", scene: Any = None):
-        if scene is not None:
-            raise NotImplementedError("scene collision is outside the IK hot path")
+        self.scene = scene
         if config.enable_T_world_base:
             raise NotImplementedError("a floating base in IKSolver is outside this build (fixed base only)")
         if config.score_terms:
@@ -113,6 +113,22 @@ class IKSolver:
                 elif t.prev_state_var is not None:
                     raise NotImplementedError("IKSolver velocity templates take prev_state_var=IKContext.PREVIOUS_STATE")
                 out.append(v)
+            elif isinstance(t, SceneCollisionTask) and t.robot is None:
+                scene = self.scene if t.scene is IKContext.SCENE else t.scene
+                if scene is None or isinstance(scene, Context) or scene.num_elements == 0:
+                    continue  # no scene: the template adds nothing (helpers/ik/ik.py:642-651)
+                si = t.scene_indices
+                if isinstance(si, Context) and si is not IKContext.SCENE_INDICES:
+                    raise NotImplementedError(f"scene_indices={si} is not an IKSolver placeholder")
+                c = SceneCollisionTask(self.robot, scene, geometry=t.geometry,
+                                       use_link_bounding_sphere_filter=t.use_link_bounding_sphere_filter,
+                                       weight=t.weight, margin=t.margin, sphere_indices=t.sphere_indices,
+                                       residual_mode=t.residual_mode, residual_eps=t.residual_eps, penalty=t.penalty,
+                                       movable_only=t.movable_only, name=t.name)
+                c.set_scene_indices(self._scene_idx if si is IKContext.SCENE_INDICES or si is None else si)
+                out.append(c)
+            elif isinstance(t, SceneCollisionTask):
+                out.append(t)  # built with a robot: passes as is
             elif isinstance(t, ConfigurationTask):
                 c = ConfigurationTask(self.robot, rest_q=None if t.rest_q_arg is IKContext.REST_Q else t.rest_q_arg,
                                       weight=t.weight, name=t.name, mask=t.mask)
@@ -131,6 +147,7 @@ class IKSolver:
         self._targets = N.DeviceArray.zeros((B, self.num_targets, 7))
         self._prev_q = N.DeviceArray.zeros((B, na))  # IKContext.PREVIOUS_STATE: zeros until a prev_state
         self._rest_q = N.DeviceArray.from_numpy(np.tile(spec.zero_q.astype(np.float32), (B, 1)))  # IKContext.REST_Q
+        self._scene_idx = N.DeviceArray.zeros(B, np.int32)  # IKContext.SCENE_INDICES
         self._terms = self._concrete_terms(self._targets)
         self._pose_terms = [t for t in self._terms if isinstance(t, _PoseTask)]
         for t in self._pose_terms:  # every stage's problem reads the one target buffer
@@ -234,7 +251,8 @@ class IKSolver:
 
     def solve(self, T_world_target: Any, prev_state: Optional[RobotState] = None,
               init_state: Optional[RobotState] = None, rest_state: Optional[RobotState] = None,
-              out_state: Optional[RobotState] = None, init_sample_range: Optional[float] = None) -> RobotState:
+              out_state: Optional[RobotState] = None, init_sample_range: Optional[float] = None,
+              scene_indices: Any = None) -> RobotState:
         """Solutions for every target, instance-major: (batch * num_solutions, dofs) (helpers/ik/ik.py:223-304).
 
         prev_state (batch,) fills IKContext.PREVIOUS_STATE and is kept for a target where it costs no more
@@ -268,6 +286,12 @@ class IKSolver:
                 raise NotImplementedError("a floating base in IKSolver is outside this build (fixed base only)")
         if rest_state is not None and rest_state.batch_size != B:
             raise ValueError(f"rest_state batch size mismatch: expected {B}, got {rest_state.batch_size}")
+        if scene_indices is not None:
+            si = N.as_device(scene_indices, np.int32)
+            if si.ndim != 1:
+                raise TypeError("scene_indices must be a 1D int32 array.")
+            if si.shape != (B,):
+                raise ValueError("scene_indices must have shape (batch_size,).")
         st = self._stream.handle
         nbytes = self._targets.nbytes
         if host:
@@ -279,6 +303,8 @@ class IKSolver:
             self._score_previous(prev_state, st)
         if rest_state is not None:
             N.check(N.lib().ik_memcpy_dtod(self._rest_q.ptr, rest_state.q.ptr, self._rest_q.nbytes, st))
+        if scene_indices is not None:
+            N.check(N.lib().ik_memcpy_dtod(self._scene_idx.ptr, si.ptr, self._scene_idx.nbytes, st))
         if init_state is not None:
             self._seed_around(init_state, self.config.sampler.scale if init_sample_range is None else init_sample_range,
                               st)

@@ -130,3 +130,43 @@ def test_lm_with_scene_collision_matches_the_oracle(gpu, panda_collision_spec, f
     assert close.mean() >= 0.85, close.mean()
     c0 = 0.5 * (oracle.residual_jacobian(rob, ot, q0, None)[0] ** 2).sum(axis=1)
     assert np.median(cost_g) < 0.1 * np.median(c0)
+
+
+def test_iksolver_with_a_scene(gpu, panda_collision_spec):
+    """IKSolver(scene=...) with a SceneCollisionTask template: targets reached, and an obstacle in one scene
+    pushes the arm out of it while the other scene (empty of it) does not; scene_indices select per target."""
+    from robokit_b200.helpers.ik import IKContext, IKSolver, IKSolverConfig
+    from robokit_b200.opt.sampler import RobertsSamplerConfig
+    from robokit_b200.robo.robot import Robot
+
+    spec = panda_collision_spec
+    robot = Robot(spec)
+    hand = spec.link_names.index("panda_hand")
+    B = 64
+    qs = robot.sample_q(B, seed=12)
+    T = robot.forward_kinematics(robot.state(qs)).get_T_world_link(hand).numpy().reshape(B, 1, 7)
+    scene = Scene(num_scenes=2)
+    # a wide slab through the workspace in scene 1 only; both scenes share a floor far below
+    scene.add(BoxGeom([[0.05, 1.0, 1.0]], [0, 0, 1], poses=[[0.25, 0.0, 0.5, 1, 0, 0, 0]]))
+    scene.add(PlaneGeom([0, 1, 2], poses=[[0, 0, -1.0, 1, 0, 0, 0]] * 2))
+    cfg = IKSolverConfig(sampler=RobertsSamplerConfig(keep_first=True, scale=1.0))
+    cfg.add(PositionTask(frame_index=IKContext.TARGET_LINKS, T_world_target=IKContext.TARGET, weight=20.0))
+    cfg.add(RotationTask(frame_index=IKContext.TARGET_LINKS, T_world_target=IKContext.TARGET, weight=10.0))
+    cfg.add(PositionLimit(weight=50.0))
+    cfg.add(SceneCollisionTask(scene=IKContext.SCENE, scene_indices=IKContext.SCENE_INDICES, weight=20.0,
+                               margin=0.01, movable_only=True))
+    ik = IKSolver(cfg, robot, "panda_hand", scene=scene)
+    free = ik.solve(T).q.numpy().copy()  # scene indices default to 0: no slab
+    assert ik.compute_metrics(robot.state(free), T).success.mean() >= 0.9
+    blocked = ik.solve(T, scene_indices=np.ones(B, np.int32)).q.numpy()
+    with pytest.raises(ValueError):
+        ik.solve(T, scene_indices=np.ones(B // 2, np.int32))
+    rob = oracle.Robot.from_spec(spec)
+    mov = np.flatnonzero(spec.collision_spheres_link_indices > 0)
+
+    def pen(q):  # deepest penetration of the slab by a movable sphere
+        c = oracle.fk(rob, q)["spheres"][:, mov]
+        d = np.max(np.abs(c - [0.25, 0.0, 0.5]) - [0.05, 1.0, 1.0], axis=2)
+        return np.maximum(0, spec.collision_sphere_radii[mov][None] - d).max(axis=1)
+
+    assert np.mean(pen(blocked) < 0.02) > np.mean(pen(free) < 0.02)
