@@ -66,6 +66,10 @@ extern "C" {
 #define IK_TERM_VELOCITY_LIMIT 7 /* w_a max(0, |q_a - prev_a| / dt - vmax_a), one row per actuated joint:
                                     VelocityLimitTask (velocity_limit_task.py:14); weights [na];
                                     d_targets = previous joints [target_rows, na]; dt, velocity_limits */
+#define IK_TERM_BASE_REF 9        /* w_k log(T_world_base T_ref^-1)_k, six rows [v; om]: the floating-base
+                                     block of SmoothnessTask / ConfigurationTask (smoothness_task.py:369-402,
+                                     configuration_task.py:337-368); weights [6];
+                                     d_targets = reference base poses [target_rows, 7]; floating base only */
 #define IK_TERM_SCENE_COLLISION 8 /* terms/dense/scene_collision_task.py:276 with primitive geometry
                                      (geom/geoms.py:372-500): one row per queried robot sphere,
                                      w * penalty(sdf(centre) - radius); weights [num_query_spheres] */

@@ -138,8 +138,12 @@ class Robot:
 class Terms:
     """A list of term dicts lowered to OrTerm structs (arrays kept alive here)."""
 
-    def __init__(self, terms: Sequence[Dict[str, Any]]):
+    def __init__(self, terms: Sequence[Any]):
         self.keep: List[np.ndarray] = []
+        flat: List[Dict[str, Any]] = []
+        for t in terms:  # a term may hold several descriptors (joint rows, then base rows)
+            flat.extend(t if isinstance(t, list) else [t])
+        terms = flat
         arr = (OrTerm * max(1, len(terms)))()
         for i, t in enumerate(terms):
             def keep(x, dt):

@@ -518,6 +518,8 @@ int or_residual_dim(const OrRobot* r, const OrTerm* terms, int32_t nterms) {
             R += r->na;
         else if (t->kind == 8)
             R += t->num_query_spheres;
+        else if (t->kind == 9)
+            R += 6;
         else if (t->kind == 4)
             R += t->pair_mode == 0 ? t->max_active_pairs : t->num_sphere_pairs;
     }
@@ -676,6 +678,33 @@ static void eval_terms(const OrRobot* r, const OrTerm* terms, int nterms, int fl
                 }
             }
             row += r->na;
+        } else if (t->kind == 9) {
+            /* smoothness_task.py:369-460, configuration_task.py:337-384: r = w (.) log(T_base T_ref^-1),
+             * base columns w (.) jlog(E) Ad(T_ref), joint columns 0 */
+            const int rows = t->target_rows > 0 ? t->target_rows : B;
+            int rep = B / rows;
+            if (rep < 1) rep = 1;
+            int rr = b / rep;
+            if (rr > rows - 1) rr = rows - 1;
+            const P7 Tr = p7_from_f(t->targets + (size_t)rr * 7);
+            const P7 Tri = inverse(&Tr);
+            const P7 E = compose(&K->base, &Tri);
+            double lg[6];
+            se3_log6(&E, lg);
+            for (int k = 0; k < 6; ++k) res[row + k] = t->weights[k] * lg[k];
+            if (J) {
+                double M1[36], M2[36];
+                se3_jlog6(&E, M1);
+                se3_adjoint6(&Tr, M2);
+                for (int i = 0; i < 6; ++i)
+                    for (int c = 0; c < D; ++c) {
+                        double v = 0.0;
+                        if (c < 6 && floating)
+                            for (int k = 0; k < 6; ++k) v += M1[6 * i + k] * M2[6 * k + c];
+                        J[(size_t)(row + i) * D + c] = t->weights[i] * v;
+                    }
+            }
+            row += 6;
         } else if (t->kind == 8) {
             /* scene_collision_task.py:34-82, 550-647 with primitive geometry */
             if (!have_C) {

@@ -37,7 +37,8 @@ typedef struct OrRobot {
 typedef struct OrTerm {
     int32_t kind; /* 1 position, 2 rotation, 3 joint limit, 4 self collision, 5 frame ("log"),
                      6 joint reference (smoothness / configuration, joints only),
-                     7 velocity limit, 8 scene collision over primitives */
+                     7 velocity limit, 8 scene collision over primitives,
+                     9 floating-base reference (targets: [target_rows, 7] poses, weights [6]) */
     int32_t num_frames;
     const int32_t* frame_links;
     const float* weights;

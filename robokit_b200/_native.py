@@ -39,6 +39,7 @@ IK_TERM_FRAME = 5
 IK_TERM_JOINT_REF = 6
 IK_TERM_VELOCITY_LIMIT = 7
 IK_TERM_SCENE_COLLISION = 8
+IK_TERM_BASE_REF = 9
 IK_PENALTY_SMOOTH, IK_PENALTY_PLAIN, IK_PENALTY_SURFACE_DISTANCE = 0, 1, 2
 IK_GEOM_BOX, IK_GEOM_SPHERE, IK_GEOM_PLANE, IK_GEOM_CAPSULE = 0, 1, 2, 3
 IK_GEOM_FLOATS = 16

@@ -83,7 +83,11 @@ def make(name: str, batch: Optional[int] = None, seed: int = 0,
 
 def oracle_terms(cfg: Config) -> list:
     """The same term list as plain dicts (the oracle's OrTerm fields)."""
-    return [t.host_desc(_Stub(cfg)) for t in cfg.terms]
+    out = []
+    for t in cfg.terms:
+        d = t.host_desc(_Stub(cfg))
+        out.extend(d if isinstance(d, list) else [d])
+    return out
 
 
 class _Stub:

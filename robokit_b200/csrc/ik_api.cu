@@ -131,6 +131,7 @@ int layout_workspace(TabHeader* h, int npose, int ncoll_slots_bytes, bool need_s
     h->w_rpose = take(std::max(h->pose_rows, 3 * npose) * 4);
     h->w_fM = take(h->nframe * 18 * 4);
     h->w_jref = take(h->njref * na * 4);
+    h->w_bref = take(h->nbref * 8 * 4);
     h->w_rlim = take(na * 4);
     // The Jacobian chunk and its row records live only inside a linearisation and
     // the FP64 factor only inside a solve: they share one region.
@@ -595,6 +596,19 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         }
         jref.push_back(e);
     }
+    // base-reference blocks
+    std::vector<BaseRefEntry> bref;
+    for (size_t ti = 0; ti < terms.size(); ++ti) {
+        const TermHost& th = terms[ti];
+        if (th.d.kind != IK_TERM_BASE_REF) continue;
+        BaseRefEntry e;
+        std::memset(&e, 0, sizeof(e));
+        e.out_row = th.row;
+        e.target_rows = th.d.target_rows;
+        for (int k = 0; k < 6; ++k) e.w[k] = th.weights[k];
+        e.ref = th.d.d_targets;
+        bref.push_back(e);
+    }
     // scene-collision terms
     std::vector<SceneEntry> scene;
     for (size_t ti = 0; ti < terms.size(); ++ti) {
@@ -662,6 +676,9 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     const int o_scene = b.add(scene.data(), scene.size() * sizeof(SceneEntry));
     b.hdr()->o_scene = o_scene;
     b.hdr()->nscene = (int)scene.size();
+    const int o_bref = b.add(bref.data(), bref.size() * sizeof(BaseRefEntry));
+    b.hdr()->o_bref = o_bref;
+    b.hdr()->nbref = (int)bref.size();
     b.hdr()->o_jref = o_jref;
     o = b.addv(limw);
     b.hdr()->o_limw = o;
@@ -680,6 +697,8 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
     for (size_t i = 0; i < coll.size(); ++i) ce[i].ws_slots = slots_off + coll_slot_rel[i];
     JointRefEntry* je = reinterpret_cast<JointRefEntry*>(b.buf.data() + o_jref);
     for (size_t i = 0; i < jref.size(); ++i) je[i].ws_ref = h->w_jref / 4 + (int)i * h->na;
+    BaseRefEntry* be = reinterpret_cast<BaseRefEntry*>(b.buf.data() + o_bref);
+    for (size_t i = 0; i < bref.size(); ++i) be[i].ws_ref = h->w_bref / 4 + 8 * (int)i;
     SceneEntry* se = reinterpret_cast<SceneEntry*>(b.buf.data() + o_scene);
     for (size_t i = 0; i < scene.size(); ++i) se[i].misc = 8 + h->ncoll + (int)i;
     // lane-per-problem layout: small systems with all-pairs collision terms only
@@ -700,7 +719,7 @@ int b200ik::host::build_tables(const RobotHost& r, int floating, const std::vect
         h->t_qp = take(std::max(h->na, 1));
         h->t_base = take(h->base_off ? 7 : 0);
         h->t_basep = take(h->base_off ? 7 : 0);
-        bool ok = h->D <= kSmallD && h->nframe == 0 && h->njref == 0 && h->nscene == 0;
+        bool ok = h->D <= kSmallD && h->nframe == 0 && h->njref == 0 && h->nscene == 0 && h->nbref == 0;
         for (size_t i = 0; i < coll.size(); ++i) {
             if (ce[i].mode != IK_PAIRS_ALL) ok = false;
             ce[i].t_mask = take((ce[i].nsp + 31) / 32);
@@ -803,6 +822,13 @@ int b200ik::host::fill_terms(const RobotHost& r, int floating, const IkTermDesc*
             const int per = d.kind == IK_TERM_FRAME ? 2 : 3;
             th.weights.assign(d.weights, d.weights + per * d.num_frames);
             th.rows = (d.kind == IK_TERM_FRAME ? 6 : 3) * d.num_frames;
+        } else if (d.kind == IK_TERM_BASE_REF) {
+            if (!floating) return fail(IK_E_INVALID, "term %d: base residuals need a floating base", i);
+            if (!d.weights) return fail(IK_E_INVALID, "term %d: base weights are NULL", i);
+            if (!d.d_targets) return fail(IK_E_INVALID, "term %d: base-reference term needs reference poses", i);
+            if (d.target_rows < 1) return fail(IK_E_INVALID, "term %d: target_rows %d", i, d.target_rows);
+            th.weights.assign(d.weights, d.weights + 6);
+            th.rows = 6;
         } else if (d.kind == IK_TERM_SCENE_COLLISION) {
             int rc = scene_records(r, d, i, th);
             if (rc) return rc;
@@ -1021,7 +1047,7 @@ int ik_problem_set_targets(IkProblem* P, int32_t term_index, const float* d_targ
     if (term_index < 0 || term_index >= (int)P->terms.size()) return fail(IK_E_INVALID, "term %d out of range", term_index);
     TermHost& th = P->terms[term_index];
     if (th.d.kind != IK_TERM_POSITION && th.d.kind != IK_TERM_ROTATION && th.d.kind != IK_TERM_FRAME &&
-        th.d.kind != IK_TERM_JOINT_REF && th.d.kind != IK_TERM_VELOCITY_LIMIT)
+        th.d.kind != IK_TERM_JOINT_REF && th.d.kind != IK_TERM_VELOCITY_LIMIT && th.d.kind != IK_TERM_BASE_REF)
         return fail(IK_E_INVALID, "term %d has no pose targets", term_index);
     if (!d_targets) return fail(IK_E_INVALID, "targets are NULL");
     th.d.d_targets = d_targets;
@@ -1126,8 +1152,9 @@ int ik_solve_persistent(IkProblem* P, int32_t batch, float* d_q, float* d_base, 
     const int G = problem_group(P);
     const int smem = smem_bytes(P->blob_bytes, P->ws_bytes, G);
     const TabHeader* th = reinterpret_cast<const TabHeader*>(P->blob.data());
-    if (th->nframe == 0 && th->njref == 0 && th->nscene == 0) {
-        // no frame, joint-reference or scene entries: the kernel without those paths (a smaller instruction footprint)
+    if (th->nframe == 0 && th->njref == 0 && th->nscene == 0 && th->nbref == 0) {
+        // no frame, joint-reference, base-reference or scene entries: the kernel without those paths
+        // (a smaller instruction footprint)
         IK_DISPATCH(G, lm_persistent_core, {
             rc = prepare_kernel(kfn, smem);
             if (rc) return rc;

@@ -194,14 +194,12 @@ __device__ __forceinline__ void m3_quat(float w, float x, float y, float z, floa
     R[6] = 2.f * (x * z - w * y); R[7] = 2.f * (y * z + w * x); R[8] = 1.f - 2.f * (x * x + y * y);
 }
 
-// Jacobian factors of a frame residual (frame_task.py:391-456): for a world twist [v; om] of a
-// tangent column the six rows are -w (.) [P v + K om; P om], where with F = T_target^-1 T_frame,
-// (w, p) its axis-angle and translation, A = Jl^-1(w)^T (so3_jac_left_inv_func,
-// lie/so3_kernels.py:14-40), B the upper-right block of the SE(3) jlog (se3_jlog_func,
-// lie/se3_kernels.py:359-428) and (t_i, R_i) = T_frame^-1 (se3_adjoint_func :314-346):
-//   P = A R_i,   K = (A hat(t_i) + B) R_i.
-__device__ __forceinline__ void frame_jacobian_factors(const Pose& Tf, const Pose& Tt, float P[9], float K[9]) {
-    const Pose F = compose(pose_inverse(Tt), Tf);
+// Jlog(F) Ad(T) = [[P, K], [0, P]] for twists [v; om]: with (w, p) the axis-angle and
+// translation of F, A = Jl^-1(w)^T (so3_jac_left_inv_func, lie/so3_kernels.py:14-40) and B the
+// upper-right block of the SE(3) jlog (se3_jlog_func, lie/se3_kernels.py:359-428), so that
+// Jlog(F) = [[A, B], [0, A]], and T = (R, t) (se3_adjoint_func :314-346):
+//   P = A R,   K = (A hat(t) + B) R.
+__device__ __forceinline__ void se3_jlog_ad(const Pose& F, const Pose& Ti, float P[9], float K[9]) {
     float ang;
     const V3 w = quat_to_axis_angle(F.w, F.i, F.j, F.k, ang);
     const V3 p{F.x, F.y, F.z};
@@ -243,7 +241,6 @@ __device__ __forceinline__ void frame_jacobian_factors(const Pose& Tf, const Pos
                 C[3 * i + j] = vv[i] * ww[j] + beta * ww[i] * pp[j] + (i == j ? wtp * beta : 0.f) + 0.5f * Hp[3 * i + j];
         m3_mul(C, A, B);
     }
-    const Pose Ti = pose_inverse(Tf);
     float R[9], Ht[9], AH[9];
     m3_quat(Ti.w, Ti.i, Ti.j, Ti.k, R);
     m3_hat(V3{Ti.x, Ti.y, Ti.z}, Ht);
@@ -252,6 +249,16 @@ __device__ __forceinline__ void frame_jacobian_factors(const Pose& Tf, const Pos
 #pragma unroll
     for (int k = 0; k < 9; ++k) AH[k] += B[k];
     m3_mul(AH, R, K);
+}
+
+// Jacobian factors of a frame residual (frame_task.py:391-456): for a world twist [v; om] of a
+// tangent column the six rows are -w (.) [P v + K om; P om], where with F = T_target^-1 T_frame,
+// (w, p) its axis-angle and translation, A = Jl^-1(w)^T (so3_jac_left_inv_func,
+// lie/so3_kernels.py:14-40), B the upper-right block of the SE(3) jlog (se3_jlog_func,
+// lie/se3_kernels.py:359-428) and (t_i, R_i) = T_frame^-1 (se3_adjoint_func :314-346):
+//   P = A R_i,   K = (A hat(t_i) + B) R_i.
+__device__ __forceinline__ void frame_jacobian_factors(const Pose& Tf, const Pose& Tt, float P[9], float K[9]) {
+    se3_jlog_ad(compose(pose_inverse(Tt), Tf), pose_inverse(Tf), P, K);
 }
 
 // ---------------------------------------------------------------------------
@@ -366,6 +373,7 @@ struct Tabs {
     IK_TAB(CollEntry, coll, o_coll)
     IK_TAB(JointRefEntry, jref, o_jref)
     IK_TAB(SceneEntry, scene, o_scene)
+    IK_TAB(BaseRefEntry, bref, o_bref)
     IK_TAB(float, limw, o_limw)
     IK_TAB(float, mask, o_mask)
     IK_TAB(uint16_t, ab, o_ab)
@@ -710,6 +718,30 @@ __device__ __forceinline__ SceneRow scene_row(const Tabs& t, const Ws& w, const 
     return o;
 }
 
+// Base-reference block at base pose Tb: weighted residual w (.) log(Tb T_ref^-1) and, when J
+// is given, its 6x6 base Jacobian w (.) Jlog(E) Ad(T_ref) (smoothness_task.py:369-460) in J[6 * k + c].
+__device__ __forceinline__ void base_ref_rows(const BaseRefEntry& be, const Ws& w, const Pose& Tb, float r[6],
+                                              float* J) {
+    const Pose Tr = pose_load(reinterpret_cast<const float*>(w.raw) + be.ws_ref);
+    const Pose E = compose(Tb, pose_inverse(Tr));
+    float lg[6], ang;
+    se3_log(E, lg, ang);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) r[k] = be.w[k] * lg[k];
+    if (!J) return;
+    float Pm[9], Km[9];
+    se3_jlog_ad(E, Tr, Pm, Km);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            J[6 * k + c] = be.w[k] * Pm[3 * k + c];
+            J[6 * k + 3 + c] = be.w[k] * Km[3 * k + c];
+            J[6 * (k + 3) + c] = 0.f;
+            J[6 * (k + 3) + 3 + c] = be.w[k + 3] * Pm[3 * k + c];
+        }
+}
+
 __device__ __forceinline__ int scene_of(const Ws& w, const SceneEntry& se) {
     return reinterpret_cast<const int*>(w.misc())[se.misc];
 }
@@ -977,6 +1009,12 @@ __device__ __forceinline__ EvalOut group_eval(const Group<G>& g, const Tabs& t, 
             reinterpret_cast<int*>(w.misc())[8 + ci] = nsl;
             o.nslots += nsl;
         }
+    }
+    // floating-base reference blocks (smoothness / rest)
+    for (int k = 0; F && base && k < h->nbref; ++k) {
+        float r[6];
+        base_ref_rows(t.bref()[k], w, pose_load(base), r, nullptr);
+        if (g.lane < 6) kadd(ks, kc, r[g.lane] * r[g.lane]);
     }
     // scene collision, scene_collision_task.py:550-592
     for (int k = 0; F && k < h->nscene; ++k) {
@@ -1328,6 +1366,18 @@ __device__ __forceinline__ void group_linearize(const Group<G>& g, const Tabs& t
                 }
             }
         }
+    }
+    // floating-base reference blocks: six rows on the base columns
+    for (int k = 0; F && base && k < h->nbref; ++k) {
+        if (g.lane < 6) {
+            float r[6], J6[36];
+            base_ref_rows(t.bref()[k], w, pose_load(base), r, J6);
+            float* J = w.Jc() + g.lane * h->Dp;
+            for (int c = 0; c < h->D; ++c) J[c] = c < 6 ? J6[6 * g.lane + c] : 0.f;
+            J[h->D] = r[g.lane];
+        }
+        g.sync();
+        group_accumulate_chunk<G>(g, t, w, 6);
     }
     // scene-collision rows with a non-zero Jacobian, compacted into chunks
     for (int k = 0; F && k < h->nscene; ++k) {

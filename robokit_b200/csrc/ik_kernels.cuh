@@ -198,6 +198,11 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 const SceneEntry& se = t.scene()[k];
                 for (int i = g.lane; i < se.nq; i += G) ro[se.out_row + i] = scene_row(t, w, se, scene_of(w, se), i).r;
             }
+            for (int k = 0; b && k < h->nbref; ++k) {
+                float r6[6];
+                base_ref_rows(t.bref()[k], w, pose_load(b), r6, nullptr);
+                if (g.lane < 6) ro[t.bref()[k].out_row + g.lane] = r6[g.lane];
+            }
         }
         float* S = ev.S;
         for (int j = g.lane; j < h->nj; j += G) {
@@ -240,6 +245,14 @@ __global__ void __launch_bounds__(kBlockThreads) resjac_kernel(const char* __res
                 const JointRefEntry& jr = t.jref()[je];
                 for (int a = g.lane; a < h->na; a += G)
                     Jo[(size_t)(jr.out_row + a) * D + boff + a] = jref_row(t, w, jr, w.q[a], a).js;
+            }
+            for (int k = 0; b && k < h->nbref; ++k) {
+                if (g.lane < 6) {
+                    float r6[6], J6[36];
+                    base_ref_rows(t.bref()[k], w, pose_load(b), r6, J6);
+                    for (int c = 0; c < D; ++c)
+                        Jo[(size_t)(t.bref()[k].out_row + g.lane) * D + c] = c < 6 ? J6[6 * g.lane + c] : 0.f;
+                }
             }
             for (int k = 0; k < h->nscene; ++k) {
                 const SceneEntry& se = t.scene()[k];

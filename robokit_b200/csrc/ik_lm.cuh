@@ -45,6 +45,14 @@ __device__ __forceinline__ void load_point(const Group<G>& g, const Tabs& t, Ws&
 template <int G>
 __device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
     const TabHeader* h = t.h;
+    for (int it = g.lane; it < h->nbref * 7; it += G) {
+        const BaseRefEntry& be = t.bref()[it / 7];
+        const int c = it % 7;
+        int rep = batch / be.target_rows;
+        if (rep < 1) rep = 1;
+        const int row = min(p / rep, be.target_rows - 1);
+        reinterpret_cast<float*>(w.raw)[be.ws_ref + c] = be.ref[(size_t)row * 7 + c];
+    }
     // the problem's scene per scene term (scene_collision_task.py:486-500: row b / (batch / rows)),
     // clamped to the scenes that exist
     for (int k = g.lane; k < h->nscene; k += G) {

@@ -570,7 +570,7 @@ int ik_server_add_type(IkServer* S, IkRobot* robot, int32_t floating_base, const
     T->params = *params;
     for (int i = 0; i < num_terms; ++i)
         if (descs[i].kind == IK_TERM_JOINT_REF || descs[i].kind == IK_TERM_VELOCITY_LIMIT ||
-            descs[i].kind == IK_TERM_SCENE_COLLISION) {
+            descs[i].kind == IK_TERM_SCENE_COLLISION || descs[i].kind == IK_TERM_BASE_REF) {
             delete T;
             return fail(IK_E_UNSUPPORTED, "term %d: joint-reference and scene terms are not served (no per-request "
                         "references or scenes)", i);

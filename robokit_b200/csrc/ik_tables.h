@@ -106,6 +106,19 @@ struct SceneEntry {
 };
 static_assert(sizeof(SceneEntry) == 64, "SceneEntry layout");
 
+// One base-reference block: rows w_k log(T_world_base T_ref^-1)_k (SmoothnessTask with a
+// floating-base previous state, smoothness_task.py:369-402, 426-460; ConfigurationTask toward a
+// rest base pose, configuration_task.py:337-384).
+struct BaseRefEntry {
+    int32_t out_row;      // first of the six rows
+    int32_t target_rows;  // rows of the reference array (broadcast rule as for pose targets)
+    int32_t ws_ref;       // workspace float offset of this problem's reference pose [8]
+    int32_t pad;
+    float w[6];
+    const float* ref;     // device [target_rows, 7]
+};
+static_assert(sizeof(BaseRefEntry) == 48, "BaseRefEntry layout");
+
 struct TabHeader {
     int32_t bytes;        // blob size, multiple of 16
     int32_t nj, nl, na, ns;
@@ -143,6 +156,10 @@ struct TabHeader {
     int32_t t_Tj, t_S, t_sph, t_tgt, t_Hs, t_Hc, t_q, t_qp, t_base, t_basep;
     int32_t nscene;       // scene-collision terms (at most IK_SCENE_MAX_TERMS)
     int32_t o_scene;      // blob offset of the SceneEntry table
+    int32_t nbref;        // base-reference blocks
+    int32_t o_bref;       // blob offset of the BaseRefEntry table
+    int32_t w_bref;       // workspace: the reference poses [nbref * 8]
+    int32_t pad2;
 };
 
 }  // namespace b200ik

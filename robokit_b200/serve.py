@@ -60,7 +60,7 @@ class IKServer:
                  active_dof_mask: Optional[np.ndarray] = None) -> int:
         """Register robot + terms + LM parameters; `slots` problems of this type may be in flight at once."""
         keep: List[Any] = []
-        descs = lower_terms(robot, list(terms), 1, floating, keep)
+        descs, ndesc = lower_terms(robot, list(terms), 1, floating, keep)
         pose_frames = [int(descs[i].num_frames) for i in range(len(terms))
                        if descs[i].kind in (N.IK_TERM_POSITION, N.IK_TERM_ROTATION, N.IK_TERM_FRAME)]
         mask = None
@@ -69,7 +69,7 @@ class IKServer:
             keep.append(mask)
         prm = lm_config.native_params()
         tid = ctypes.c_int32(0)
-        N.check(N.lib().ik_server_add_type(self.handle, robot.handle, int(bool(floating)), descs, len(terms),
+        N.check(N.lib().ik_server_add_type(self.handle, robot.handle, int(bool(floating)), descs, ndesc,
                                            N.np_ptr(mask), ctypes.byref(prm), int(slots), ctypes.byref(tid)))
         self.types.append(_TypeInfo(robot, robot.spec.num_actuated_joints, bool(floating), pose_frames, int(slots),
                                     keep))

@@ -246,6 +246,33 @@ def _ref_rows(ref: Any, na: int) -> Any:
     return a
 
 
+def _pose_rows(T: Any) -> Any:
+    """Base poses as [rows, 7] [x y z qw qx qy qz]: a DeviceArray (read in place) or float32 numpy."""
+    if isinstance(T, N.DeviceArray) or hasattr(T, "__cuda_array_interface__"):
+        d = N.as_device(T, np.float32)
+        if d.size % 7 or d.size == 0:
+            raise ValueError(f"base poses of shape {d.shape} are not rows of 7")
+        return d.reshape((d.size // 7, 7))
+    a = np.asarray(T, np.float32)
+    if a.shape[-2:] == (4, 4):
+        from ..geom import _poses_vec7
+
+        return _poses_vec7(a, a.reshape(-1, 4, 4).shape[0])
+    return np.ascontiguousarray(a.reshape(-1, 7))
+
+
+def _base_desc(weights: np.ndarray, ref: Any, host: bool) -> Dict[str, Any]:
+    """Six rows w (.) log(T_world_base T_ref^-1) (kind IK_TERM_BASE_REF)."""
+    if host:
+        r = ref.numpy() if isinstance(ref, N.DeviceArray) else np.asarray(ref, np.float32)
+        return dict(kind=N.IK_TERM_BASE_REF, weights=weights, targets=r, target_rows=r.shape[0])
+    d = ref if isinstance(ref, N.DeviceArray) else N.DeviceArray.from_numpy(np.asarray(ref, np.float32))
+    return dict(kind=N.IK_TERM_BASE_REF, weights=weights, targets=d)
+
+
+_IDENTITY_POSE = np.array([[0, 0, 0, 1, 0, 0, 0]], np.float32)
+
+
 class _JointRefTask(ResidualTask):
     """r_a = w_a (q_a - ref_a) over the actuated joints: a diagonal Jacobian block of w.
 
@@ -295,19 +322,17 @@ class _JointRefTask(ResidualTask):
 
 
 class SmoothnessTask(_JointRefTask):
-    """Penalise change from a previous joint state, w (q - q_prev) (smoothness_task.py:22-460).
-
-    Joints only: a floating-base previous state (whose base residual is an SE(3)
-    log) and the warm-up weight ramp are outside the IK hot path.  Without a
-    previous state the term adds zero rows, as the reference's does."""
+    """Penalise change from a previous state, w (q - q_prev) on the joints and, with a floating-base
+    previous state (or a base_weight), w_b (.) log(T_world_base T_prev^-1) on the base
+    (smoothness_task.py:22-460).  Base weights default to the first joint's weight.  Without a
+    previous state the term adds zero rows, as the reference's does.  The warm-up weight ramp is not
+    supported."""
 
     def __init__(self, robot: Any = None, prev_var: Any = None, weight: Union[float, Sequence[float]] = 1.0,
                  base_weight: Optional[Union[float, Sequence[float]]] = None, name: str = "", warmup_frames: int = 0,
                  frame: Any = None):
         if warmup_frames and frame is not None:
             raise NotImplementedError("the warm-up weight ramp is outside the IK hot path")
-        if base_weight is not None or getattr(prev_var, "has_floating_base", False):
-            raise NotImplementedError("base smoothness residuals are outside the IK hot path (joints only)")
         self.name = name
         self.weight = weight
         self.base_weight = base_weight
@@ -315,10 +340,46 @@ class SmoothnessTask(_JointRefTask):
         self.robot = robot
         self.prev_var = prev_var
         self._prev_q: Any = None
+        self._prev_base: Any = None
+        self._include_base = base_weight is not None or bool(getattr(prev_var, "has_floating_base", False))
         if prev_var is not None and not isinstance(prev_var, Context):
             self._prev_q = _ref_rows(prev_var.q, prev_var.spec.num_actuated_joints)
             if isinstance(self._prev_q, N.DeviceArray):  # the reference clones the state (smoothness_task.py:57)
                 self._prev_q = self._prev_q.clone()
+            if prev_var.has_floating_base:
+                self._prev_base = _pose_rows(prev_var.T_world_base)
+                if isinstance(self._prev_base, N.DeviceArray):
+                    self._prev_base = self._prev_base.clone()
+
+    @property
+    def residual_dim(self) -> int:
+        return self.robot.spec.num_actuated_joints + (6 if self._include_base else 0)
+
+    def _base_weights(self, na: int) -> np.ndarray:
+        w = np.zeros(6, np.float32)
+        if self._prev_q is None:
+            return w
+        if self.base_weight is not None:
+            w[:] = self.base_weight
+        else:
+            jw = super()._joint_weights(na)
+            w[:] = jw[0] if na else 1.0
+        return w
+
+    def _descs(self, var: Any, host: bool) -> Any:
+        d = (_JointRefTask.host_desc if host else _JointRefTask.native_desc)(self, var)
+        if not self._include_base:
+            return d
+        if not var.has_floating_base or (self._prev_q is not None and self._prev_base is None):
+            raise ValueError("SmoothnessTask is configured with base residuals but var/prev_var has no floating base.")
+        ref = self._prev_base if self._prev_base is not None else _IDENTITY_POSE
+        return [d, _base_desc(self._base_weights(var.spec.num_actuated_joints), ref, host)]
+
+    def native_desc(self, var: Any) -> Any:
+        return self._descs(var, False)
+
+    def host_desc(self, var: Any) -> Any:
+        return self._descs(var, True)
 
     @property
     def active(self) -> bool:
@@ -342,13 +403,18 @@ class SmoothnessTask(_JointRefTask):
 
     def set_prev_state(self, prev_state: Any) -> None:
         """Copy a new previous state in place; a new row count rebuilds (smoothness_task.py:111-120)."""
-        if getattr(prev_state, "has_floating_base", False):
-            raise NotImplementedError("base smoothness residuals are outside the IK hot path (joints only)")
         new = _ref_rows(prev_state.q, prev_state.spec.num_actuated_joints)
-        if isinstance(self._prev_q, N.DeviceArray) and self._prev_q.shape == new.shape:
+        newb = _pose_rows(prev_state.T_world_base) if prev_state.has_floating_base else None
+        if (isinstance(self._prev_q, N.DeviceArray) and self._prev_q.shape == new.shape and
+                (newb is None) == (self._prev_base is None) and
+                (newb is None or (isinstance(self._prev_base, N.DeviceArray) and self._prev_base.shape == newb.shape))):
             self._prev_q.assign(new)
+            if newb is not None:
+                self._prev_base.assign(newb)
             return
         self._prev_q = new.clone() if isinstance(new, N.DeviceArray) else new
+        self._prev_base = None if newb is None else (newb.clone() if isinstance(newb, N.DeviceArray) else newb)
+        self._include_base = self._include_base or newb is not None
         self._touch()
 
 
@@ -357,13 +423,13 @@ class ConfigurationTask(_JointRefTask):
 
     ``rest_q`` is "midrange" (the joint-limit midpoints), an array of one or more
     rows, or None (the zero configuration); ``mask`` scales each joint's weight.
-    The base rest pose (an SE(3) log residual) is outside the IK hot path."""
+    With ``T_world_base_rest`` (rows of [x y z qw qx qy qz] or 4x4 poses) six more
+    rows w_b (.) log(T_world_base T_rest^-1) bias a floating base toward it
+    (base_weight, default 1); ``include_joints=False`` keeps only those."""
 
     def __init__(self, robot: Any = None, rest_q: Any = None, T_world_base_rest: Any = None,
                  weight: Union[float, Sequence[float]] = 1.0, base_weight: Any = None, include_joints: bool = True,
                  var_key: Any = None, name: str = "", mask: Any = None):
-        if T_world_base_rest is not None or base_weight is not None:
-            raise NotImplementedError("base rest residuals are outside the IK hot path (joints only)")
         if isinstance(rest_q, str) and rest_q != "midrange":
             raise ValueError(f"Unsupported rest_q: {rest_q}")
         if isinstance(mask, Context):
@@ -376,6 +442,12 @@ class ConfigurationTask(_JointRefTask):
         self.rest_q_arg = rest_q
         self.robot = robot
         self._rest: Any = None
+        self._base_rest_arg = T_world_base_rest
+        self._base_rest: Any = None
+        if T_world_base_rest is not None and not isinstance(T_world_base_rest, Context):
+            self._base_rest = _pose_rows(T_world_base_rest)
+            if isinstance(self._base_rest, N.DeviceArray):  # the reference clones it (configuration_task.py:141)
+                self._base_rest = self._base_rest.clone()
         if var_key is not None:
             self.var_key = var_key
 
@@ -391,6 +463,37 @@ class ConfigurationTask(_JointRefTask):
         if self.mask is not None:
             w *= self.mask
         return w
+
+    @property
+    def _has_base(self) -> bool:
+        return self._base_rest_arg is not None
+
+    @property
+    def residual_dim(self) -> int:
+        na = self.robot.spec.num_actuated_joints
+        return (na if self.include_joints or not self._has_base else 0) + (6 if self._has_base else 0)
+
+    def _descs(self, var: Any, host: bool) -> Any:
+        d = (_JointRefTask.host_desc if host else _JointRefTask.native_desc)(self, var)
+        if not self._has_base:
+            return d
+        if isinstance(self._base_rest_arg, Context):
+            raise ValueError("T_world_base_rest is a placeholder: build the term through a helper or give it")
+        if not var.has_floating_base:
+            raise ValueError("ConfigurationTask has a rest base pose but the state has no floating base")
+        if self._base_rest is None:
+            self._base_rest = _pose_rows(self._base_rest_arg)
+        bw = np.ones(6, np.float32)
+        if self.base_weight is not None:
+            bw[:] = self.base_weight
+        out = [d] if self.include_joints else []
+        return out + [_base_desc(bw, self._base_rest, host)]
+
+    def native_desc(self, var: Any) -> Any:
+        return self._descs(var, False)
+
+    def host_desc(self, var: Any) -> Any:
+        return self._descs(var, True)
 
     def _reference(self, na: int) -> Any:
         if self._rest is not None:
@@ -420,7 +523,14 @@ class ConfigurationTask(_JointRefTask):
     def set_target(self, rest_q: Any = None, T_world_base_rest: Any = None) -> None:
         """Overwrite the rest joints in place; a new row count rebuilds (configuration_task.py:153-177)."""
         if T_world_base_rest is not None:
-            raise NotImplementedError("base rest residuals are outside the IK hot path (joints only)")
+            new_b = _pose_rows(T_world_base_rest)
+            cur_b = self._base_rest
+            if isinstance(cur_b, N.DeviceArray) and cur_b.shape == new_b.shape:
+                cur_b.assign(new_b)
+            else:
+                self._base_rest_arg = T_world_base_rest
+                self._base_rest = new_b
+                self._touch()
         if rest_q is None:
             return
         na = self.robot.spec.num_actuated_joints if self.robot is not None else np.asarray(rest_q).shape[-1]

@@ -115,7 +115,7 @@ def _destroy_problem(handle: int) -> None:
 
 def lower_terms(robot: Any, terms: List[ResidualTask], capacity: int, floating: bool,
                 keep: List[Any]) -> Any:
-    """IkTermDesc array for `terms`; the host arrays it points at are appended to `keep`."""
+    """(IkTermDesc array, descriptor count) for `terms`; the host arrays it points at are appended to `keep`."""
 
     def arr(x: Any, dt: Any) -> Optional[int]:
         if x is None:
@@ -126,10 +126,13 @@ def lower_terms(robot: Any, terms: List[ResidualTask], capacity: int, floating: 
         keep.append(a)
         return a.ctypes.data
 
-    descs = (N.IkTermDesc * max(1, len(terms)))()
     var_stub = _VarStub(robot, capacity, floating)
-    for i, t in enumerate(terms):
+    flat: List[Dict[str, Any]] = []
+    for t in terms:  # a term may lower to several descriptors (joint rows, then base rows)
         d = t.native_desc(var_stub)
+        flat.extend(d if isinstance(d, list) else [d])
+    descs = (N.IkTermDesc * max(1, len(flat)))()
+    for i, d in enumerate(flat):
         descs[i].kind = d["kind"]
         descs[i].num_frames = d.get("num_frames", 0)
         descs[i].frame_links = arr(d.get("frame_links"), np.int32)
@@ -165,7 +168,7 @@ def lower_terms(robot: Any, terms: List[ResidualTask], capacity: int, floating: 
                 keep.append(si)
                 descs[i].d_scene_indices = si.ptr
                 descs[i].scene_rows = si.shape[0]
-    return descs
+    return descs, len(flat)
 
 
 class NativeProblem:
@@ -176,13 +179,13 @@ class NativeProblem:
         import weakref
 
         self.keep: List[Any] = []
-        descs = lower_terms(robot, terms, capacity, floating, self.keep)
+        descs, ndesc = lower_terms(robot, terms, capacity, floating, self.keep)
         mask = None
         if active_dof_mask is not None:
             mask = np.ascontiguousarray(active_dof_mask, np.float32)
             self.keep.append(mask)
         h = ctypes.c_void_p(0)
-        N.check(N.lib().ik_problem_create(robot.handle, int(capacity), int(bool(floating)), descs, len(terms),
+        N.check(N.lib().ik_problem_create(robot.handle, int(capacity), int(bool(floating)), descs, ndesc,
                                           N.np_ptr(mask), ctypes.byref(h)))
         self.handle = h.value
         self.robot = robot

@@ -182,3 +182,76 @@ def test_iksolver_smooth_preset_stays_near_the_previous_state(gpu, panda_arm_spe
     assert ik.compute_metrics(robot.state(a), T).success.mean() >= 0.9
     # the smoothness pull keeps the redundant arm near prev more often than an unregularised solve
     assert np.median(np.abs(a - prev).max(axis=1)) <= np.median(np.abs(b - prev).max(axis=1))
+
+
+def _unit_poses(rng, n, scale=0.2):
+    p = rng.normal(size=(n, 7)).astype(np.float32)
+    p[:, :3] *= scale
+    p[:, 3] += 2.0
+    p[:, 3:] /= np.linalg.norm(p[:, 3:], axis=1, keepdims=True)
+    return p
+
+
+def test_base_reference_rows_match_the_oracle(gpu, panda_spec):
+    """Floating-base blocks of SmoothnessTask (previous base pose) and ConfigurationTask (rest base pose):
+    residual and Jacobian rows against the oracle."""
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_spec)
+    rng = np.random.default_rng(17)
+    B = 48
+    na = panda_spec.num_actuated_joints
+    q = (panda_spec.midrange_q + rng.normal(0, 0.3, (B, na))).astype(np.float32)
+    base = _unit_poses(rng, B)
+    prev_base = _unit_poses(rng, B)
+    rest_base = _unit_poses(rng, 2)  # 2 rows shared by B // 2 problems each
+    terms = [SmoothnessTask(robot, prev_var=robot.state(q + 0.1, prev_base), weight=0.5,
+                            base_weight=[1, 2, 3, 0.5, 0.25, 4]),
+             ConfigurationTask(robot, rest_q="midrange", T_world_base_rest=rest_base, weight=0.2, base_weight=1.5),
+             ConfigurationTask(robot, T_world_base_rest=rest_base[:1], include_joints=False)]
+    st = robot.state(q, base)
+    vv = VarValues({VarKey.ROBOT: st})
+    D = st.tangent_dim
+    R = sum(t.residual_dim for t in terms)
+    assert R == (na + 6) * 2 + 6
+    r = N.DeviceArray.zeros((B, R))
+    J = N.DeviceArray.zeros((B, R, D))
+    off = 0
+    for t in terms:
+        t.compute_weighted_residual(vv, out_residual=r, row_offset=off)
+        t.compute_weighted_jacobian(vv, out_jacobian=J, row_offset=off)
+        off += t.residual_dim
+    ro, Jo = oracle.residual_jacobian(oracle.Robot.from_spec(panda_spec),
+                                      oracle.Terms([t.host_desc(_view(panda_spec, B, True)) for t in terms]), q, base)
+    np.testing.assert_allclose(r.numpy(), ro, rtol=1e-4, atol=2e-5)
+    np.testing.assert_allclose(J.numpy(), Jo, rtol=1e-3, atol=1e-4)
+
+
+def test_lm_with_base_smoothness_matches_the_oracle(gpu, panda_arm_spec):
+    """A floating-base arm reaching FK targets with base smoothness toward a previous base pose: per-problem
+    costs agree with the oracle."""
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_arm_spec)
+    hand = panda_arm_spec.link_names.index("panda_hand")
+    B = 128
+    rng = np.random.default_rng(5)
+    qs = robot.sample_q(B, seed=41)
+    base_s = _unit_poses(rng, B, 0.1)
+    T = robot.forward_kinematics(robot.state(qs, base_s)).get_T_world_link(hand).numpy().reshape(B, 1, 7)
+    lo, hi = panda_arm_spec.float32_actuated_limits().T
+    q0 = np.clip(qs + rng.normal(0, 0.2, qs.shape), lo, hi).astype(np.float32)
+    prev = robot.state(q0.copy(), base_s + np.r_[0.03, -0.02, 0.01, 0, 0, 0, 0].astype(np.float32))
+    terms = [PositionTask(robot, hand, T, weight=10.0), RotationTask(robot, hand, T, weight=5.0),
+             SmoothnessTask(robot, prev_var=prev, weight=0.2, base_weight=2.0)]
+    opt = LMOptimizer(terms, LMOptimizerConfig(max_iter=30, lm_lambda=1e-2, lambda_factor=2.0,
+                                               early_stopping_interval=0, form="persistent"))
+    st = robot.state(q0, base_s.copy())
+    opt.solve(VarValues({VarKey.ROBOT: st}))
+    rob = oracle.Robot.from_spec(panda_arm_spec)
+    ot = oracle.Terms([t.host_desc(_view(panda_arm_spec, B, True)) for t in terms])
+    o = oracle.solve(rob, ot, oracle.params(max_iter=30, lambda_init=1e-2, lambda_factor=2.0), q0, base_s, threads=8)
+    cost_g = 0.5 * (oracle.residual_jacobian(rob, ot, st.q.numpy(), st.T_world_base.numpy())[0] ** 2).sum(axis=1)
+    cost_o = 0.5 * (oracle.residual_jacobian(rob, ot, o["q"], o["base"])[0] ** 2).sum(axis=1)
+    close = np.abs(cost_g - cost_o) <= 1e-3 * np.maximum(1e-3, cost_o)
+    assert close.mean() >= 0.85, close.mean()

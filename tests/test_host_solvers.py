@@ -110,11 +110,27 @@ def test_joint_reference_terms_host_side(panda_spec):
     tmpl = SmoothnessTask(prev_var=IKContext.PREVIOUS_STATE, weight=0.1)
     assert tmpl.active and tmpl.robot is None
     with pytest.raises(NotImplementedError):
-        SmoothnessTask(_Robot(), base_weight=1.0)
-    with pytest.raises(NotImplementedError):
         SmoothnessTask(_Robot(), warmup_frames=5, frame=IKContext.TARGET)
-    with pytest.raises(NotImplementedError):
-        ConfigurationTask(_Robot(), T_world_base_rest=np.zeros(7))
+    # base blocks: six more rows on a floating base, refused on a fixed one
+    class _VF:
+        spec, batch_size, has_floating_base = panda_spec, 4, True
+
+    sb = SmoothnessTask(_Robot(), base_weight=2.0, weight=0.5)
+    assert sb.residual_dim == na + 6
+    with pytest.raises(ValueError, match="no floating base"):
+        sb.host_desc(_V)
+    jd, bd = sb.host_desc(_VF)
+    assert bd["kind"] == N.IK_TERM_BASE_REF and not np.any(bd["weights"])  # no previous state yet
+    cb = ConfigurationTask(_Robot(), T_world_base_rest=[[0.1, 0, 0, 1, 0, 0, 0]], base_weight=3.0)
+    assert cb.residual_dim == na + 6
+    jd, bd = cb.host_desc(_VF)
+    assert jd["kind"] == N.IK_TERM_JOINT_REF and np.all(bd["weights"] == 3.0) and bd["targets"].shape == (1, 7)
+    only = ConfigurationTask(_Robot(), T_world_base_rest=np.eye(4), include_joints=False)
+    (bd,) = only.host_desc(_VF)
+    assert only.residual_dim == 6 and np.all(bd["weights"] == 1.0)
+    np.testing.assert_allclose(bd["targets"], [[0, 0, 0, 1, 0, 0, 0]], atol=1e-7)
+    with pytest.raises(ValueError):
+        cb.host_desc(_V)
     with pytest.raises(ValueError):
         ConfigurationTask(_Robot(), rest_q="zero")
     assert [type(t).__name__ for t in presets.smooth.terms] == ["PositionTask", "RotationTask", "PositionLimit",

@@ -347,3 +347,53 @@ def test_oracle_scene_selection_and_query_order(panda_collision_spec):
     np.testing.assert_allclose(r[1], expect, rtol=1e-9, atol=1e-7)
     np.testing.assert_allclose(r[2:], np.broadcast_to(1e6 - spec.collision_sphere_radii.astype(np.float32), (2, ns)),
                                rtol=1e-6)
+
+
+def _qmul(a, b):
+    w1, x1, y1, z1 = a
+    w2, x2, y2, z2 = b
+    return np.array([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2, w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                     w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2, w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2])
+
+
+def _qrot(q, v):
+    return _qmul(_qmul(q, np.r_[0.0, v]), q * [1, -1, -1, -1])[1:]
+
+
+def test_oracle_base_reference_term_matches_finite_differences(panda_spec):
+    """Floating-base reference rows w (.) log(T_base T_ref^-1): the base block of the Jacobian agrees with
+    central differences under the right-multiplied base update, the joint columns are zero, and the rows
+    vanish at the reference."""
+    spec = panda_spec
+    rob = oracle.Robot.from_spec(spec)
+    na = spec.num_actuated_joints
+    q = spec.midrange_q[None].astype(np.float32)
+    ref = np.array([[0.2, -0.1, 0.3, 0.8, 0.3, -0.4, 0.2]])
+    ref[:, 3:] /= np.linalg.norm(ref[:, 3:])
+    w = np.array([1.0, 2.0, 0.5, 1.5, 0.7, 3.0])
+    terms = oracle.Terms([dict(kind=9, weights=w, targets=ref.astype(np.float32), target_rows=1)])
+    assert oracle.residual_dim(rob, terms) == 6
+    base = np.array([0.5, 0.3, -0.2, 0.6, -0.2, 0.5, 0.4])
+    base[3:] /= np.linalg.norm(base[3:])
+    r, J = oracle.residual_jacobian(rob, terms, q, base[None].astype(np.float32))
+    assert J.shape == (1, 6, 6 + na) and not np.any(J[0][:, 6:])
+    eps = 1e-4
+
+    def moved(c, s):
+        t, qb = base[:3].copy(), base[3:].copy()
+        if c < 3:
+            e = np.zeros(3)
+            e[c] = s * eps
+            t = t + _qrot(qb, e)
+        else:
+            e = np.zeros(3)
+            e[c - 3] = 1.0
+            qb = _qmul(qb, np.r_[np.cos(s * eps / 2), np.sin(s * eps / 2) * e])
+        return np.r_[t, qb][None].astype(np.float64)
+
+    for c in range(6):
+        rp, _ = oracle.residual_jacobian(rob, terms, q, moved(c, 1))
+        rm, _ = oracle.residual_jacobian(rob, terms, q, moved(c, -1))
+        np.testing.assert_allclose(J[0][:, c], (rp[0] - rm[0]) / (2 * eps), atol=2e-3)
+    r0, _ = oracle.residual_jacobian(rob, terms, q, ref.astype(np.float32))
+    assert np.abs(r0).max() < 1e-6
