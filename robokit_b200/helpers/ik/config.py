@@ -25,7 +25,7 @@ class IKContext(Context):
     REST_Q = 4
     """Rest configurations (batch, dofs): the zero configuration until solve(rest_state=...)."""
     REST_BASE = 5
-    """Rest base poses; a fixed base has none (templates on it are not supported here)."""
+    """Rest base poses (batch,): identity until solve(rest_state=...); None for a fixed base."""
     NUM_SOLUTIONS = 6
     """Solutions each target returns."""
     OPTIMIZATION_TERMS = 7

@@ -37,6 +37,9 @@ from ...terms.task import Context
 from .config import IKContext, IKSolverConfig
 
 
+_IDENTITY7 = np.array([0, 0, 0, 1, 0, 0, 0], np.float32)
+
+
 @dataclass
 class IKMetrics:
     """Per target and target link: position error [m], angle error [rad]; per target: success."""
@@ -50,8 +53,6 @@ class IKSolver:
     def __init__(self, config: IKSolverConfig, robot: Any, target_links: Union[str, int, Sequence[Union[str, int]]],
                  device: Any = "cuda", scene: Any = None):
         self.scene = scene
-        if config.enable_T_world_base:
-            raise NotImplementedError("a floating base in IKSolver is outside this build (fixed base only)")
         if config.score_terms:
             raise NotImplementedError("score terms are outside this build (candidates rank by cost)")
         if device is not None and not str(device).startswith("cuda"):
@@ -64,7 +65,42 @@ class IKSolver:
         self.num_targets = len(self.target_links)
         self.widths = config.solver.num_candidates
         self.lm_configs = config.solver.optimizers
+        self.floating = bool(config.enable_T_world_base)
+        self._joint_mask = np.ones(robot.spec.num_actuated_joints, np.float32)
+        self._base_mask = np.asarray(config.base_active_mask, np.float32).copy()
         self._batch = None
+
+    # --- active degrees of freedom (helpers/ik/ik.py:200-216) --------------------------------
+    def set_active_joint_mask(self, joint_mask: Sequence[float]) -> None:
+        """Which actuated joints move (1.0) or stay locked (0.0); the next solve rebuilds the stages."""
+        m = np.asarray(joint_mask, np.float32).reshape(-1)
+        if m.shape != self._joint_mask.shape:
+            raise ValueError(f"joint_mask length {m.size} != {self._joint_mask.size}")
+        self._joint_mask[:] = m
+        self._rebuild()
+
+    def set_active_base_mask(self, base_mask: Sequence[float]) -> None:
+        """Active (1.0) / locked (0.0) base DOFs [x, y, z, roll, pitch, yaw]; needs enable_T_world_base=True."""
+        if not self.floating:
+            raise ValueError("set_active_base_mask requires enable_T_world_base=True")
+        if len(base_mask) != 6:
+            raise ValueError(f"base_mask length {len(base_mask)} != 6")
+        self._base_mask[:] = np.asarray(base_mask, np.float32)
+        self._rebuild()
+
+    def _rebuild(self) -> None:
+        if self._batch is not None:
+            self._pending_batch = self._batch
+            self._batch = None
+
+    def _dof_mask(self) -> Optional[np.ndarray]:
+        m = np.concatenate([self._base_mask, self._joint_mask]) if self.floating else self._joint_mask.copy()
+        return None if np.all(m == 1.0) else m
+
+    def _state(self, rows: int, q: Optional[np.ndarray] = None) -> RobotState:
+        na = self.num_joints
+        q = np.zeros((rows, na), np.float32) if q is None else q
+        return self.robot.state(q, np.tile(_IDENTITY7, (rows, 1)) if self.floating else None)
 
     # --- sizes -------------------------------------------------------------------------
     @property
@@ -101,7 +137,7 @@ class IKSolver:
             elif isinstance(t, SmoothnessTask):
                 s = SmoothnessTask(self.robot, weight=t.weight, name=t.name)
                 if t.prev_var is IKContext.PREVIOUS_STATE:
-                    s.bind_previous(self._prev_q)
+                    s.bind_previous(self._prev_q, self._prev_base)
                 elif t.prev_var is not None:
                     raise NotImplementedError("IKSolver smoothness templates take prev_var=IKContext.PREVIOUS_STATE")
                 out.append(s)
@@ -130,8 +166,16 @@ class IKSolver:
             elif isinstance(t, SceneCollisionTask):
                 out.append(t)  # built with a robot: passes as is
             elif isinstance(t, ConfigurationTask):
+                rb = t._base_rest_arg if self.floating else None  # a fixed base drops the base rows
+                if rb is IKContext.REST_BASE:
+                    rb = self._rest_base
+                elif isinstance(rb, Context):
+                    raise NotImplementedError(f"T_world_base_rest={rb} is not an IKSolver placeholder")
                 c = ConfigurationTask(self.robot, rest_q=None if t.rest_q_arg is IKContext.REST_Q else t.rest_q_arg,
-                                      weight=t.weight, name=t.name, mask=t.mask)
+                                      T_world_base_rest=rb, weight=t.weight, base_weight=t.base_weight,
+                                      include_joints=t.include_joints, name=t.name, mask=t.mask)
+                if rb is self._rest_base and rb is not None:
+                    c._base_rest = self._rest_base  # read in place
                 if t.rest_q_arg is IKContext.REST_Q:
                     c.bind_rest(self._rest_q)
                 elif isinstance(t.rest_q_arg, Context):
@@ -146,6 +190,9 @@ class IKSolver:
         na = spec.num_actuated_joints
         self._targets = N.DeviceArray.zeros((B, self.num_targets, 7))
         self._prev_q = N.DeviceArray.zeros((B, na))  # IKContext.PREVIOUS_STATE: zeros until a prev_state
+        ident = np.tile(_IDENTITY7, (B, 1))
+        self._prev_base = N.DeviceArray.from_numpy(ident) if self.floating else None
+        self._rest_base = N.DeviceArray.from_numpy(ident) if self.floating else None  # IKContext.REST_BASE
         self._rest_q = N.DeviceArray.from_numpy(np.tile(spec.zero_q.astype(np.float32), (B, 1)))  # IKContext.REST_Q
         self._scene_idx = N.DeviceArray.zeros(B, np.int32)  # IKContext.SCENE_INDICES
         self._terms = self._concrete_terms(self._targets)
@@ -153,22 +200,27 @@ class IKSolver:
         for t in self._pose_terms:  # every stage's problem reads the one target buffer
             t.bind_targets(self._targets)
         self._stages = []
+        self._mask = self._dof_mask()
         for k, (width, lm) in enumerate(zip(self.widths, self.lm_configs)):
             iters = self.config.solver.stages[k].iters
-            state = self.robot.state(np.zeros((B * width, na), np.float32))
+            state = self._state(B * width)
             opt = None
             if iters > 0:
                 cfg = replace(lm, max_iter=iters, early_stopping_interval=0, form="persistent")
-                opt = LMOptimizer(self._terms, cfg)
+                opt = LMOptimizer(self._terms, cfg, active_dof_mask=self._mask)
                 opt.reset(VarValues({VarKey.ROBOT: state}))
             self._stages.append((width, iters, state, opt))
         C0 = self.widths[0]
         lim = spec.float32_actuated_limits()
         self._range = (lim[:, 1] - lim[:, 0]).astype(np.float32)
-        self._sampler = RobertsSampler(C0, na, self.config.sampler.seed, self.config.sampler.keep_first)
+        # one Roberts spread over the whole tangent (base twist first), helpers/ik/ik.py:512-526
+        Dt = (6 if self.floating else 0) + na
+        self._sampler = RobertsSampler(C0, Dt, self.config.sampler.seed, self.config.sampler.keep_first)
         self._mid = N.DeviceArray.from_numpy(np.tile(spec.midrange_q.astype(np.float32), (B * C0, 1)))
-        # spread around the midrange (fixed, read by the captured graph) and around an init_state
-        self._noise_mid = N.DeviceArray.from_numpy(self._sampler.tangent(B, self._range))
+        self._base0 = N.DeviceArray.from_numpy(np.tile(_IDENTITY7, (B * C0, 1))) if self.floating else None
+        # spread around the midrange (fixed, read by the captured graph; the base stays at identity) and
+        # around an init_state
+        self._noise_mid = N.DeviceArray.from_numpy(self._sampler.tangent(B, self._tangent_scale(1.0, None)))
         self._noise_scale = None
         self._noise = None
         self._cost = [N.DeviceArray.zeros(B * w) for w in self.widths]
@@ -178,19 +230,34 @@ class IKSolver:
         self._scorer: Optional[LMOptimizer] = None  # prices a previous state (built on the first one)
         self._batch = B
 
+    def _tangent_scale(self, q_range: Any, base_range: Optional[Sequence[float]]) -> np.ndarray:
+        """Spread of the candidate noise: base translation (only around an init_state), joints x their mask."""
+        s = np.asarray(q_range, np.float32) * self._range * self._joint_mask
+        if not self.floating:
+            return s.astype(np.float32)
+        b = np.zeros(6, np.float32)
+        if base_range is not None:
+            b[:3] = np.asarray(base_range, np.float32) * self._base_mask[:3]
+        return np.concatenate([b, s]).astype(np.float32)
+
     def _score_previous(self, prev_state: RobotState, stream: int) -> None:
         """Cost of prev_state under the solve's terms, its smoothness rows zero (helpers/ik/ik.py:257-270)."""
         B, na = self._batch, self.num_joints
         if self._scorer is None:
-            self._prev_save = self.robot.state(np.zeros((B, na), np.float32))
+            self._prev_save = self._state(B)
             self._prev_cost = N.DeviceArray.zeros(B)
-            self._scorer = LMOptimizer(self._terms, LMOptimizerConfig(max_iter=0, form="persistent"))
+            self._scorer = LMOptimizer(self._terms, LMOptimizerConfig(max_iter=0, form="persistent"),
+                                       active_dof_mask=self._mask)
             self._scorer.reset(VarValues({VarKey.ROBOT: self._prev_save}))
             self._score_params = self._scorer.config.native_params()
         N.check(N.lib().ik_memcpy_dtod(self._prev_save.q.ptr, prev_state.q.ptr, self._prev_q.nbytes, stream))
+        if self.floating:
+            src = self._prev_base  # the previous base if one was given, else what the placeholder holds
+            N.check(N.lib().ik_memcpy_dtod(self._prev_save.T_world_base.ptr, src.ptr, src.nbytes, stream))
         sc = self._scorer
         sc._slice(B)
-        N.check(N.lib().ik_solve_persistent(sc.problem.handle, B, self._prev_save.q.ptr, None,
+        N.check(N.lib().ik_solve_persistent(sc.problem.handle, B, self._prev_save.q.ptr,
+                                            self._prev_save.T_world_base.ptr if self.floating else None,
                                             ctypes.byref(self._score_params), self._prev_cost.ptr, sc.lm.ptr,
                                             sc.iterations.ptr, sc.status.ptr, stream))
 
@@ -201,8 +268,9 @@ class IKSolver:
         N.synchronize()
 
     # --- solve ---------------------------------------------------------------------------
-    def _seed_around(self, init_state: RobotState, q_range: Union[float, Sequence[float]], stream: int) -> None:
-        """Candidates spread around init_state's joints (helpers/ik/ik.py:486-540)."""
+    def _seed_around(self, init_state: RobotState, q_range: Union[float, Sequence[float]], stream: int,
+                     base_range: Optional[Sequence[float]] = None) -> None:
+        """Candidates spread around init_state's joints and base (helpers/ik/ik.py:486-540)."""
         B, C0 = self._batch, self.widths[0]
         na = self.num_joints
         state = self._stages[0][2]
@@ -210,14 +278,22 @@ class IKSolver:
             raise ValueError(f"init_state batch size {init_state.batch_size} != {B}")
         rep = np.repeat(np.arange(B, dtype=np.int32), C0)
         center = N.DeviceArray.from_numpy(init_state.q.numpy()[rep])
+        cbase = None
+        if self.floating:
+            b = init_state.T_world_base.numpy() if init_state.has_floating_base else np.tile(_IDENTITY7, (B, 1))
+            cbase = N.DeviceArray.from_numpy(np.ascontiguousarray(b.reshape(B, 7)[rep], np.float32))
         if C0 == 1:
             N.check(N.lib().ik_memcpy_dtod(state.q.ptr, center.ptr, center.nbytes, stream))
+            if cbase is not None:
+                N.check(N.lib().ik_memcpy_dtod(state.T_world_base.ptr, cbase.ptr, cbase.nbytes, stream))
         else:
-            scale = np.asarray(q_range, np.float32) * self._range
+            br = self.config.base_init_sample_range if base_range is None else base_range
+            scale = self._tangent_scale(q_range, br)
             if self._noise_scale is None or not np.array_equal(scale, self._noise_scale):
                 self._noise = N.DeviceArray.from_numpy(self._sampler.tangent(B, scale))
                 self._noise_scale = scale
-            N.check(N.lib().ik_integrate(B * C0, na, 0, center.ptr, None, self._noise.ptr, None, state.q.ptr, None,
+            N.check(N.lib().ik_integrate(B * C0, na, int(self.floating), center.ptr, N.ptr(cbase), self._noise.ptr,
+                                         None, state.q.ptr, N.ptr(state.T_world_base) if self.floating else None,
                                          stream))
         N.check(N.lib().ik_clamp_q(B * C0, na, state.q.ptr, self.robot.limits_device().ptr, None, stream))
         N.check(N.lib().ik_stream_synchronize(stream))  # `center` is freed on return
@@ -226,8 +302,9 @@ class IKSolver:
         """Seed from the midrange, run every stage, select between stages: device work only, on `stream`."""
         B, C0, na = self._batch, self.widths[0], self.num_joints
         q0 = self._stages[0][2]
-        N.check(N.lib().ik_integrate(B * C0, na, 0, self._mid.ptr, None, self._noise_mid.ptr, None, q0.q.ptr, None,
-                                     stream))
+        N.check(N.lib().ik_integrate(B * C0, na, int(self.floating), self._mid.ptr, N.ptr(self._base0),
+                                     self._noise_mid.ptr, None, q0.q.ptr,
+                                     q0.T_world_base.ptr if self.floating else None, stream))
         N.check(N.lib().ik_clamp_q(B * C0, na, q0.q.ptr, self.robot.limits_device().ptr, None, stream))
         self._run_stages(stream)
 
@@ -237,22 +314,26 @@ class IKSolver:
             if opt is not None:
                 n = B * width
                 opt._slice(n)
-                N.check(N.lib().ik_solve_persistent(opt.problem.handle, n, state.q.ptr, None,
+                N.check(N.lib().ik_solve_persistent(opt.problem.handle, n, state.q.ptr,
+                                                    state.T_world_base.ptr if self.floating else None,
                                                     ctypes.byref(self._params[k]), self._cost[k].ptr, opt.lm.ptr,
                                                     opt.iterations.ptr, opt.status.ptr, stream))
             elif k == 0:
                 raise NotImplementedError("a first stage without iterations needs a scoring pass")
             if k + 1 < len(self._stages):
                 nxt_w, _, nxt_state, _ = self._stages[k + 1]
-                N.check(N.lib().ik_select_best(B, width, nxt_w, self._cost[k].ptr, state.q.ptr, None, na,
-                                               nxt_state.q.ptr, None, self._cost[k + 1].ptr, None, stream))
+                fb = self.floating
+                N.check(N.lib().ik_select_best(B, width, nxt_w, self._cost[k].ptr, state.q.ptr,
+                                               state.T_world_base.ptr if fb else None, na, nxt_state.q.ptr,
+                                               nxt_state.T_world_base.ptr if fb else None, self._cost[k + 1].ptr,
+                                               None, stream))
         for _, _, state, _ in self._stages:
             state.invalidate()
 
     def solve(self, T_world_target: Any, prev_state: Optional[RobotState] = None,
               init_state: Optional[RobotState] = None, rest_state: Optional[RobotState] = None,
               out_state: Optional[RobotState] = None, init_sample_range: Optional[float] = None,
-              scene_indices: Any = None) -> RobotState:
+              scene_indices: Any = None, base_init_sample_range: Optional[Sequence[float]] = None) -> RobotState:
         """Solutions for every target, instance-major: (batch * num_solutions, dofs) (helpers/ik/ik.py:223-304).
 
         prev_state (batch,) fills IKContext.PREVIOUS_STATE and is kept for a target where it costs no more
@@ -273,6 +354,8 @@ class IKSolver:
             raise ValueError(f"Target count ({T.shape[1] if T.ndim == 3 else '?'}) must match IK target count "
                              f"({self.num_targets})")
         B = T.shape[0]
+        if self._batch is None and getattr(self, "_pending_batch", None) not in (None, B):
+            raise ValueError(f"Batch size mismatch: expected {self._pending_batch}, got {B}")
         if self._batch is None:
             self._build(B)
         elif B != self._batch:
@@ -282,8 +365,6 @@ class IKSolver:
                 raise ValueError("prev_state requires an IK final stage with num_candidates=1.")
             if prev_state.batch_size != B:
                 raise ValueError(f"prev_state batch size mismatch: expected {B}, got {prev_state.batch_size}")
-            if prev_state.has_floating_base:
-                raise NotImplementedError("a floating base in IKSolver is outside this build (fixed base only)")
         if rest_state is not None and rest_state.batch_size != B:
             raise ValueError(f"rest_state batch size mismatch: expected {B}, got {rest_state.batch_size}")
         if scene_indices is not None:
@@ -300,14 +381,20 @@ class IKSolver:
             N.check(N.lib().ik_memcpy_dtod(self._targets.ptr, T.ptr, nbytes, st))
         if prev_state is not None:
             N.check(N.lib().ik_memcpy_dtod(self._prev_q.ptr, prev_state.q.ptr, self._prev_q.nbytes, st))
+            if self.floating and prev_state.has_floating_base:
+                N.check(N.lib().ik_memcpy_dtod(self._prev_base.ptr, prev_state.T_world_base.ptr,
+                                               self._prev_base.nbytes, st))
             self._score_previous(prev_state, st)
         if rest_state is not None:
             N.check(N.lib().ik_memcpy_dtod(self._rest_q.ptr, rest_state.q.ptr, self._rest_q.nbytes, st))
+            if self.floating and rest_state.has_floating_base:
+                N.check(N.lib().ik_memcpy_dtod(self._rest_base.ptr, rest_state.T_world_base.ptr,
+                                               self._rest_base.nbytes, st))
         if scene_indices is not None:
             N.check(N.lib().ik_memcpy_dtod(self._scene_idx.ptr, si.ptr, self._scene_idx.nbytes, st))
         if init_state is not None:
             self._seed_around(init_state, self.config.sampler.scale if init_sample_range is None else init_sample_range,
-                              st)
+                              st, base_init_sample_range)
             self._run_stages(st)
         elif self.config.solver.cuda_graph_mode == "full":
             if self._graph is None:
@@ -319,11 +406,15 @@ class IKSolver:
             self._device_body(st)
         final = self._stages[-1][2]
         if prev_state is not None:
+            fb = self.floating
             N.check(N.lib().ik_keep_previous(B, self.num_joints, self._prev_cost.ptr, self._cost[-1].ptr,
-                                             self._prev_save.q.ptr, None, final.q.ptr, None, st))
+                                             self._prev_save.q.ptr, self._prev_save.T_world_base.ptr if fb else None,
+                                             final.q.ptr, final.T_world_base.ptr if fb else None, st))
         N.check(N.lib().ik_stream_synchronize(st))
         if out_state is not None:
             out_state.q.assign(final.q)
+            if self.floating and out_state.has_floating_base:
+                out_state.T_world_base.assign(final.T_world_base)
             out_state.invalidate()
             return out_state
         return final

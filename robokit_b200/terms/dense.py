@@ -396,9 +396,13 @@ class SmoothnessTask(_JointRefTask):
         self.weight = weight
         self._touch()
 
-    def bind_previous(self, prev_q: N.DeviceArray) -> None:
-        """Read the previous joints from `prev_q` [rows, na] in place from now on."""
+    def bind_previous(self, prev_q: N.DeviceArray, prev_base: Optional[N.DeviceArray] = None) -> None:
+        """Read the previous joints from `prev_q` [rows, na] (and base poses from `prev_base` [rows, 7], which
+        adds the base rows) in place from now on."""
         self._prev_q = prev_q
+        if prev_base is not None:
+            self._prev_base = prev_base
+            self._include_base = True
         self._touch()
 
     def set_prev_state(self, prev_state: Any) -> None:
