@@ -321,7 +321,38 @@ class _JointRefTask(ResidualTask):
         return dict(kind=N.IK_TERM_JOINT_REF, weights=self._joint_weights(na), targets=ref, target_rows=ref.shape[0])
 
 
-class SmoothnessTask(_JointRefTask):
+class _PrevStateEval:
+    """The reference's evaluation signature with an optional previous state for this call only
+    (smoothness_task.py:171-300, velocity_limit_task.py:99-185)."""
+
+    def _with_prev(self, fn: Any, var_values: Any, prev_var: Any, out: Any, row_offset: int) -> Any:
+        if prev_var is None:
+            return fn(var_values, out, row_offset)
+        saved = (self._prev_q, getattr(self, "_prev_base", None))
+        self._prev_q = None  # fresh copies: a buffer bound in place is left as it is
+        if hasattr(self, "_prev_base"):
+            self._prev_base = None
+        self.set_prev_state(prev_var)
+        try:
+            return fn(var_values, out, row_offset)
+        finally:
+            self._prev_q = saved[0]
+            if hasattr(self, "_prev_base"):
+                self._prev_base = saved[1]
+            self._touch()
+
+    def compute_weighted_residual(self, var_values: Any, prev_var: Any = None, out_residual: Any = None,
+                                  row_offset: int = 0) -> Any:
+        return self._with_prev(super().compute_weighted_residual, var_values, prev_var, out_residual, row_offset)
+
+    def compute_weighted_jacobian(self, var_values: Any, prev_var: Any = None, out_jacobian: Any = None,
+                                  row_offset: int = 0) -> Any:
+        return self._with_prev(super().compute_weighted_jacobian, var_values, prev_var, out_jacobian, row_offset)
+
+    compute_weighted_jacobian_analytic = compute_weighted_jacobian
+
+
+class SmoothnessTask(_PrevStateEval, _JointRefTask):
     """Penalise change from a previous state, w (q - q_prev) on the joints and, with a floating-base
     previous state (or a base_weight), w_b (.) log(T_world_base T_prev^-1) on the base
     (smoothness_task.py:22-460).  Base weights default to the first joint's weight.  Without a
@@ -418,8 +449,7 @@ class SmoothnessTask(_JointRefTask):
             return
         self._prev_q = new.clone() if isinstance(new, N.DeviceArray) else new
         self._prev_base = None if newb is None else (newb.clone() if isinstance(newb, N.DeviceArray) else newb)
-        self._include_base = self._include_base or newb is not None
-        self._touch()
+        self._touch()  # the row layout stays as built: base rows only if configured (smoothness_task.py:111-120)
 
 
 class ConfigurationTask(_JointRefTask):
@@ -551,7 +581,7 @@ class ConfigurationTask(_JointRefTask):
         self._touch()
 
 
-class VelocityLimitTask(_JointRefTask):
+class VelocityLimitTask(_PrevStateEval, _JointRefTask):
     """Penalise joint speeds above their limits relative to a previous state,
     w max(0, |q - q_prev| / dt - v_max) (velocity_limit_task.py:14-232).
 
