@@ -215,7 +215,8 @@ class IKSolver:
         self._range = (lim[:, 1] - lim[:, 0]).astype(np.float32)
         # one Roberts spread over the whole tangent (base twist first), helpers/ik/ik.py:512-526
         Dt = (6 if self.floating else 0) + na
-        self._sampler = RobertsSampler(C0, Dt, self.config.sampler.seed, self.config.sampler.keep_first)
+        self._sampler = RobertsSampler(C0, np.ones(Dt, np.float32), self.config.sampler.seed,
+                                       self.config.sampler.keep_first)
         self._mid = N.DeviceArray.from_numpy(np.tile(spec.midrange_q.astype(np.float32), (B * C0, 1)))
         self._base0 = N.DeviceArray.from_numpy(np.tile(_IDENTITY7, (B * C0, 1))) if self.floating else None
         # spread around the midrange (fixed, read by the captured graph; the base stays at identity) and

@@ -120,3 +120,25 @@ def test_init_state_seeds_around_a_previous_solution(gpu, panda_arm_spec):
     assert m.success.mean() >= 0.95
     with pytest.raises(ValueError, match="init_state batch size"):
         ik.solve(T, init_state=robot.state(first.q.numpy()[:8]))
+
+
+def test_roberts_sampler_fill_and_sample(gpu, panda_arm_spec):
+    """tests/opt/test_sampler.py:27-54 on device arrays: fill tiles the scaled offsets, rejects a wrong width,
+    and sample() spreads a state in place."""
+    from robokit_b200 import _native as N
+    from robokit_b200.opt.sampler import RobertsSampler, RobertsSamplerConfig
+    from robokit_b200.robo.robot import Robot
+
+    s = RobertsSampler(num_candidates=4, scale=[0.5, 0.5], keep_first=True)
+    t = N.DeviceArray.zeros((8, 2))
+    s.fill(t)
+    np.testing.assert_array_equal(t.numpy(), s.tangent(2))
+    with pytest.raises(ValueError, match="tangent_dim"):
+        s.fill(N.DeviceArray.zeros((4, 3)))
+    robot = Robot(panda_arm_spec)
+    q = np.tile(panda_arm_spec.midrange_q, (8, 1)).astype(np.float32)
+    vv = VarValues({VarKey.ROBOT: robot.state(q)})
+    smp = RobertsSamplerConfig(scale=0.1, keep_first=True).build(vv, 4)
+    smp.sample(vv)
+    moved = vv.get(VarKey.ROBOT).q.numpy()
+    np.testing.assert_allclose(moved, q + smp.tangent(2), atol=1e-6)

@@ -30,7 +30,7 @@ def test_roberts_sequence():
 
 
 def test_roberts_sampler_keep_first_and_tiling():
-    s = RobertsSampler(4, 2, keep_first=True)
+    s = RobertsSampler(4, [1.0, 1.0], keep_first=True)
     assert np.all(s.offsets[0] == 0) and np.all(s.offsets[1] == -0.5)
     t = s.tangent(3, np.array([2.0, 1.0], np.float32))
     assert t.shape == (12, 2)
@@ -216,3 +216,43 @@ def test_scene_geometry_and_term_host_side(panda_collision_spec):
     with pytest.raises(ValueError, match="weight shape"):
         SceneCollisionTask(_Robot(), s, weight=[1.0, 2.0])
     assert not SceneCollisionTask(_Robot(), Scene(1)).active
+
+
+class TestRobertsSamplerReference:
+    """tests/opt/test_sampler.py:17-70 (TestRobertsSampler), on the host spread that fill() uploads."""
+
+    @staticmethod
+    def _fill(num_candidates=4, batch=2, scale=(0.5, 0.5), **kw):
+        return RobertsSampler(num_candidates=num_candidates, scale=scale, **kw).tangent(batch)
+
+    def test_shape_and_bounds(self):
+        noise = self._fill()
+        assert noise.shape == (8, 2) and np.abs(noise).max() <= 0.25
+
+    def test_scale_is_per_column(self):
+        noise = self._fill(scale=(1.0, 0.0))
+        assert np.abs(noise[:, 1]).max() == 0.0 and np.abs(noise[:, 0]).max() > 0.0
+
+    def test_every_instance_gets_the_same_seed_offsets(self):
+        noise = self._fill(num_candidates=4, batch=3)
+        np.testing.assert_array_equal(noise[0:4], noise[4:8])
+        np.testing.assert_array_equal(noise[0:4], noise[8:12])
+
+    def test_keep_first_leaves_candidate_zero_untouched(self):
+        noise = self._fill(keep_first=True)
+        np.testing.assert_array_equal(noise[0], np.zeros(2))
+        assert np.abs(noise[1:4]).max() > 0.0
+
+    def test_seed_shifts_the_sequence(self):
+        assert not np.array_equal(self._fill(seed=0), self._fill(seed=7))
+
+    def test_covers_more_evenly_than_random(self):
+        cells = lambda pts: len({(int(x * 8), int(y * 8)) for x, y in pts})  # noqa: E731
+        assert cells(roberts_samples(64, 2)) > cells(np.random.default_rng(0).random((64, 2)))
+
+    def test_scale_assign_and_config_build(self):
+        s = RobertsSampler(4, (1.0, 1.0))
+        s.scale.assign(np.array([0.0, 2.0], np.float32))
+        assert np.abs(s.tangent(1)[:, 0]).max() == 0.0
+        with pytest.raises(ValueError):
+            s.scale.assign([1.0])
