@@ -759,11 +759,19 @@ class SceneCollisionTask(ResidualTask):
     def set_scene_indices(self, scene_indices: Any) -> None:
         """The scene of each problem row, int32 (scene_collision_task.py:412-437); read in place when on the device."""
         if isinstance(scene_indices, N.DeviceArray) or hasattr(scene_indices, "__cuda_array_interface__"):
-            d = N.as_device(scene_indices, np.int32)
+            try:
+                d = N.as_device(scene_indices, np.int32)
+            except TypeError as e:
+                raise TypeError(f"scene_indices must be a 1D int32 array ({e}).") from None
         else:
-            d = N.DeviceArray.from_numpy(np.ascontiguousarray(scene_indices, np.int32).reshape(-1))
-        if d.ndim != 1 or d.shape[0] < 1:
-            raise ValueError("scene_indices must be a non-empty 1D int32 array.")
+            a = np.asarray(scene_indices)
+            if a.dtype != np.int32:
+                raise TypeError(f"scene_indices must be a 1D int32 array, got {a.dtype}.")
+            d = N.DeviceArray.from_numpy(np.ascontiguousarray(a))
+        if d.ndim != 1:
+            raise TypeError("scene_indices must be a 1D int32 array.")
+        if d.shape[0] < 1:
+            raise ValueError("scene_indices must not be empty.")
         self.scene_indices = d
         self._scene_idx_dev = d
         self._touch()

@@ -170,3 +170,83 @@ def test_iksolver_with_a_scene(gpu, panda_collision_spec):
         return np.maximum(0, spec.collision_sphere_radii[mov][None] - d).max(axis=1)
 
     assert np.mean(pen(blocked) < 0.02) > np.mean(pen(free) < 0.02)
+
+
+# tests/terms/test_scene_collision_task.py:524-640 (TestWarpSceneCollisionTaskMultiScene), with primitive planes
+# and boxes in place of the meshes: a multi-scene task with a batch partition equals the concatenation of
+# single-scene tasks, and bad scene indices are refused.
+_QY90 = [0.7071067811865476, 0.0, 0.7071067811865476, 0.0]  # local z onto world x
+
+
+def _plane_x(x, offsets):
+    return PlaneGeom(offsets, poses=[[x, 0.0, 0.0, *_QY90]] * int(offsets[-1]))
+
+
+def _scene_single(k):
+    s = Scene(1)
+    if k == 0:
+        s.add(_plane_x(0.3, [0, 1])).add(BoxGeom([[0.2, 0.2, 0.2]], [0, 1], poses=[[0.6, 0, 0.4, 1, 0, 0, 0]]))
+        s.add(SphereGeom([0.1], [0, 1]))
+    elif k == 1:
+        s.add(_plane_x(0.5, [0, 1])).add(BoxGeom([[0.1, 0.1, 0.1]], [0, 1]))
+    else:
+        s.add(BoxGeom([[0.15, 0.15, 0.15]], [0, 1], poses=[[0.3, 0.1, 0.5, 1, 0, 0, 0]]))
+    return s
+
+
+def _scene_multi(n):
+    s = Scene(n)
+    planes = [0.3, 0.5][: min(n, 2)]
+    off_p = [0, 1, 2] + [2] * (n - 2)
+    s.add(PlaneGeom(off_p[: n + 1], poses=[[x, 0.0, 0.0, *_QY90] for x in planes]))
+    boxes, off_b = [[0.6, 0, 0.4, 1, 0, 0, 0], [0, 0, 0, 1, 0, 0, 0]], [0, 1, 2]
+    he = [[0.2, 0.2, 0.2], [0.1, 0.1, 0.1]]
+    if n == 3:
+        boxes.append([0.3, 0.1, 0.5, 1, 0, 0, 0])
+        he.append([0.15, 0.15, 0.15])
+        off_b = [0, 1, 2, 3]
+    s.add(BoxGeom(he, off_b, poses=boxes))
+    s.add(SphereGeom([0.1], [0, 1] + [1] * (n - 1)))
+    return s
+
+
+def _run_scene_task(robot, q, scene, scene_indices=None):
+    st = robot.state(q=q)
+    task = SceneCollisionTask(robot=robot, scene=scene, scene_indices=scene_indices, weight=1.0, margin=0.02,
+                              residual_mode="abs")
+    vv = VarValues({VarKey.ROBOT: st})
+    return task.compute_weighted_residual(vv).numpy(), task.compute_weighted_jacobian_analytic(vv).numpy()
+
+
+@pytest.mark.parametrize("partition", [[0, 2], [0, 1, 5]])
+def test_multi_scene_matches_per_scene_tasks(gpu, panda_collision_spec, partition):
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_collision_spec)
+    rng = np.random.RandomState(len(partition))
+    B = 4 if len(partition) == 2 else 6
+    q = (rng.randn(B, robot.num_actuated_joints) * 0.1 + robot.spec.midrange_q).astype(np.float32)
+    bounds = np.r_[partition, B]
+    idx = np.repeat(np.arange(len(partition), dtype=np.int32), np.diff(bounds))
+    r_multi, j_multi = _run_scene_task(robot, q, _scene_multi(len(partition)), N.DeviceArray.from_numpy(idx))
+    parts = [_run_scene_task(robot, q[lo:hi], _scene_single(k)) for k, (lo, hi) in
+             enumerate(zip(bounds[:-1], bounds[1:])) if hi > lo]
+    r_ref = np.concatenate([p[0] for p in parts])
+    j_ref = np.concatenate([p[1] for p in parts])
+    assert r_multi.shape == r_ref.shape and j_multi.shape == j_ref.shape
+    assert np.allclose(r_multi, r_ref, atol=1e-5, rtol=1e-5)
+    assert np.allclose(j_multi, j_ref, atol=1e-5, rtol=1e-5)
+
+
+def test_rejects_bad_scene_indices(gpu, panda_collision_spec):
+    from robokit_b200.robo.robot import Robot
+
+    robot = Robot(panda_collision_spec)
+    scene = _scene_multi(2)
+    q = np.zeros((4, robot.num_actuated_joints), np.float32)
+    with pytest.raises(TypeError, match="int32"):
+        _run_scene_task(robot, q, scene, N.DeviceArray.zeros(4, np.float32))
+    with pytest.raises(TypeError, match="1D"):
+        _run_scene_task(robot, q, scene, N.DeviceArray.zeros((4, 1), np.int32))
+    with pytest.raises(ValueError, match="batch_size"):
+        _run_scene_task(robot, q, scene, N.DeviceArray.zeros(3, np.int32))
