@@ -465,7 +465,7 @@ def ik_solver_bench(batches=(1, 10, 100, 1000, 2000), runs: int = 5) -> dict:
             sol = ik.solve(T)
             N.synchronize()
             times.append((time.perf_counter() - t0) * 1e3)
-            m = ik.compute_metrics(sol, T)
+            m = ik.compute_metrics_numpy(sol, T)
             ok = m.success
             succ.append(100.0 * ok.mean())
             if ok.any():

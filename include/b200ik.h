@@ -358,6 +358,20 @@ int ik_copy_rows(int32_t rows, int32_t width, const float* d_src, int64_t src_st
 int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, const float* d_src, float* d_dst,
                         void* stream);
 
+/* Cost of every row of a residual block, the reference's
+ * aggregate_residuals_to_costs_kernel (opt/optimizer.py:21-33):
+ * d_out[r] = (accumulate ? d_out[r] : 0) + sum_{i<width} d_x[r*stride + i]^2,
+ * one FP32 running sum per row in column order.  Used by IKSolver.compute_costs
+ * (helpers/ik/ik.py:373-385, opt/population_solver.py:555-574). */
+int ik_row_sumsq(int32_t rows, int32_t width, const float* d_x, int64_t stride, float* d_out, int32_t accumulate,
+                 void* stream);
+
+/* Homogeneous transforms, 4x4 row-major floats, to and from poses
+ * [x, y, z, qw, qx, qy, qz] with qw >= 0: the se3_from_matrix / se3_to_matrix
+ * conversions of IKSolver.solve_torch (helpers/ik/ik.py:306-347). */
+int ik_pose_from_matrix(int32_t n, const float* d_mats, float* d_poses, void* stream);
+int ik_matrix_from_pose(int32_t n, const float* d_poses, float* d_mats, void* stream);
+
 /* Keep the best `keep` of every instance's `num_candidates` candidates by cost
  * (ascending, equal costs in candidate order, NaN last), the select of
  * PopulationSolver (opt/population_solver.py:490-528).  Inputs are

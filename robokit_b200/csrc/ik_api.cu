@@ -1458,6 +1458,32 @@ int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, cons
     return check_launch();
 }
 
+int ik_row_sumsq(int32_t rows, int32_t width, const float* d_x, int64_t stride, float* d_out, int32_t accumulate,
+                 void* stream) {
+    if (rows < 0 || width < 0) return fail(IK_E_INVALID, "negative size");
+    if (stride < width) return fail(IK_E_INVALID, "stride < width");
+    if (rows == 0) return IK_OK;
+    if (!d_out || (width > 0 && !d_x)) return fail(IK_E_INVALID, "NULL array");
+    row_sumsq_kernel<<<elementwise_grid(rows), 256, 0, S(stream)>>>(rows, width, d_x, stride, d_out, accumulate ? 1 : 0);
+    return check_launch();
+}
+
+int ik_pose_from_matrix(int32_t n, const float* d_mats, float* d_poses, void* stream) {
+    if (n < 0) return fail(IK_E_INVALID, "negative size");
+    if (n == 0) return IK_OK;
+    if (!d_mats || !d_poses) return fail(IK_E_INVALID, "NULL array");
+    pose_from_matrix_kernel<<<elementwise_grid(n), 256, 0, S(stream)>>>(n, d_mats, d_poses);
+    return check_launch();
+}
+
+int ik_matrix_from_pose(int32_t n, const float* d_poses, float* d_mats, void* stream) {
+    if (n < 0) return fail(IK_E_INVALID, "negative size");
+    if (n == 0) return IK_OK;
+    if (!d_mats || !d_poses) return fail(IK_E_INVALID, "NULL array");
+    matrix_from_pose_kernel<<<elementwise_grid(n), 256, 0, S(stream)>>>(n, d_poses, d_mats);
+    return check_launch();
+}
+
 int ik_select_best(int32_t batch, int32_t num_candidates, int32_t keep, const float* d_cost, const float* d_q,
                    const float* d_base, int32_t num_actuated, float* d_q_out, float* d_base_out, float* d_cost_out,
                    int32_t* d_index_out, void* stream) {

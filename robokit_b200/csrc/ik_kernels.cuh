@@ -542,6 +542,79 @@ __global__ void masked_copy_rows_kernel(int rows, int width, const int* mask, co
     }
 }
 
+// Row cost: out[r] = (acc ? out[r] : 0) + sum_i x[r, i]^2, summed in column order in FP32 with one fused
+// multiply-add per element, one thread per row (opt/optimizer.py:21-33).
+__global__ void row_sumsq_kernel(int rows, int width, const float* x, long long stride, float* out, int acc) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows; r += (long long)gridDim.x * blockDim.x) {
+        const float* row = x + r * stride;
+        float c = acc ? out[r] : 0.f;
+        float s = 0.f;
+        for (int i = 0; i < width; ++i) s = fmaf(row[i], row[i], s);
+        out[r] = c + s;
+    }
+}
+
+// Homogeneous 4x4 row-major matrices <-> poses [x, y, z, qw, qx, qy, qz] (xform se3_from_matrix /
+// se3_to_matrix, used by IKSolver.solve_torch, helpers/ik/ik.py:306-347).  The quaternion follows
+// Shepperd's method (J. Guidance and Control 1(3), 1978): the largest of 1 + trace and 1 + 2 R_ii - trace
+// picks the component computed from a square root, the others come from off-diagonal sums and
+// differences; the result is normalised with qw >= 0.
+__global__ void pose_from_matrix_kernel(int n, const float* mats, float* poses) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float* m = mats + i * 16;
+        const float r00 = m[0], r01 = m[1], r02 = m[2], r10 = m[4], r11 = m[5], r12 = m[6];
+        const float r20 = m[8], r21 = m[9], r22 = m[10];
+        const float tr = r00 + r11 + r22;
+        float q[4];  // w, x, y, z
+        if (tr >= r00 && tr >= r11 && tr >= r22) {
+            const float s = 2.f * sqrtf(fmaxf(1.f + tr, 0.f));
+            q[0] = 0.25f * s;
+            q[1] = (r21 - r12) / s;
+            q[2] = (r02 - r20) / s;
+            q[3] = (r10 - r01) / s;
+        } else if (r00 >= r11 && r00 >= r22) {
+            const float s = 2.f * sqrtf(fmaxf(1.f + r00 - r11 - r22, 0.f));
+            q[0] = (r21 - r12) / s;
+            q[1] = 0.25f * s;
+            q[2] = (r01 + r10) / s;
+            q[3] = (r02 + r20) / s;
+        } else if (r11 >= r22) {
+            const float s = 2.f * sqrtf(fmaxf(1.f + r11 - r00 - r22, 0.f));
+            q[0] = (r02 - r20) / s;
+            q[1] = (r01 + r10) / s;
+            q[2] = 0.25f * s;
+            q[3] = (r12 + r21) / s;
+        } else {
+            const float s = 2.f * sqrtf(fmaxf(1.f + r22 - r00 - r11, 0.f));
+            q[0] = (r10 - r01) / s;
+            q[1] = (r02 + r20) / s;
+            q[2] = (r12 + r21) / s;
+            q[3] = 0.25f * s;
+        }
+        float nrm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if (q[0] < 0.f) nrm = -nrm;
+        float* p = poses + i * 7;
+        p[0] = m[3];
+        p[1] = m[7];
+        p[2] = m[11];
+        for (int k = 0; k < 4; ++k) p[3 + k] = q[k] / nrm;
+    }
+}
+
+__global__ void matrix_from_pose_kernel(int n, const float* poses, float* mats) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float* p = poses + i * 7;
+        float w = p[3], x = p[4], y = p[5], z = p[6];
+        const float inv = 1.f / sqrtf(w * w + x * x + y * y + z * z);
+        w *= inv, x *= inv, y *= inv, z *= inv;
+        float* m = mats + i * 16;
+        m[0] = 1.f - 2.f * (y * y + z * z), m[1] = 2.f * (x * y - w * z), m[2] = 2.f * (x * z + w * y), m[3] = p[0];
+        m[4] = 2.f * (x * y + w * z), m[5] = 1.f - 2.f * (x * x + z * z), m[6] = 2.f * (y * z - w * x), m[7] = p[1];
+        m[8] = 2.f * (x * z - w * y), m[9] = 2.f * (y * z + w * x), m[10] = 1.f - 2.f * (x * x + y * y), m[11] = p[2];
+        m[12] = 0.f, m[13] = 0.f, m[14] = 0.f, m[15] = 1.f;
+    }
+}
+
 __global__ void keep_previous_kernel(int batch, int na, const float* prev_cost, const float* cost, const float* prev_q,
                                      const float* prev_base, float* q, float* base) {
     const int w = na + (base ? 7 : 0);

@@ -65,13 +65,31 @@ class IKSolverConfig:
             raise ValueError("base_active_mask requires enable_T_world_base=True")
 
     def add(self, term: ResidualTask, *, name: Optional[str] = None) -> "IKSolverConfig":
-        if name is not None:
-            term.name = name
+        """Append an optimization term; without `name` it is called `<cost_name>_<n>`, the first n free."""
+        self._assign_name(term, name)
         self.terms.append(term)
         return self
 
     def add_score(self, term: ResidualTask, *, name: Optional[str] = None) -> "IKSolverConfig":
-        if name is not None:
-            term.name = name
+        """Append a term that ranks candidates at every select (by the sum of its squared residuals) without
+        entering the optimization (helpers/ik/config.py:53-54)."""
+        self._assign_name(term, name)
         self.score_terms.append(term)
         return self
+
+    def task(self, name: str) -> ResidualTask:
+        """The term added under `name` (helpers/ik/config.py:84-89)."""
+        for t in (*self.terms, *self.score_terms):
+            if t.name == name:
+                return t
+        raise KeyError(f"No IK term named {name!r}.")
+
+    def _assign_name(self, term: ResidualTask, name: Optional[str]) -> None:
+        if name is not None:
+            term.name = name
+            return
+        taken = {t.name for t in (*self.terms, *self.score_terms)}
+        n = 0
+        while f"{term.cost_name}_{n}" in taken:
+            n += 1
+        term.name = f"{term.cost_name}_{n}"

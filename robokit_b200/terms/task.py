@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import abc
 import ctypes
+import re
 from enum import Enum
 from typing import Any, Dict, List, Optional
 
@@ -27,6 +28,12 @@ class Context(Enum):
 class Task(abc.ABC):
     name: str = ""
     var_key = VarKey.ROBOT
+
+    @property
+    def cost_name(self) -> str:
+        """The class name in snake case (PositionTask -> position_task): the key of this term's cost in cost
+        reports and the stem of the names a config gives its terms (terms/task.py:89-93)."""
+        return re.sub(r"(?<!^)(?=[A-Z])", "_", type(self).__name__).lower()
 
 
 class ResidualTask(Task):

@@ -49,7 +49,7 @@ def test_basic_preset_solves_panda_targets(gpu, panda_arm_spec):
     T = _targets(robot, 128, 42, link)
     sol = ik.solve(T)
     assert sol.q.shape == (128, 7)
-    m = ik.compute_metrics(sol, T)
+    m = ik.compute_metrics_numpy(sol, T)
     assert m.success.mean() >= 0.95, m.success.mean()
     # the metrics kernel against the FP64 oracle
     rob = oracle.Robot.from_spec(panda_arm_spec)
@@ -58,7 +58,7 @@ def test_basic_preset_solves_panda_targets(gpu, panda_arm_spec):
     np.testing.assert_allclose(m.orientation_error_rad, re, atol=2e-4)
     # a second solve on new targets reuses the buffers
     T2 = _targets(robot, 128, 43, link)
-    assert ik.compute_metrics(ik.solve(T2), T2).success.mean() >= 0.95
+    assert ik.compute_metrics_numpy(ik.solve(T2), T2).success.mean() >= 0.95
     with pytest.raises(ValueError, match="Batch size mismatch"):
         ik.solve(T2[:64])
 
@@ -116,7 +116,7 @@ def test_init_state_seeds_around_a_previous_solution(gpu, panda_arm_spec):
     first = ik.solve(T)
     prev = robot.state(first.q.numpy())
     again = ik.solve(T, init_state=prev, init_sample_range=0.05)
-    m = ik.compute_metrics(again, T)
+    m = ik.compute_metrics_numpy(again, T)
     assert m.success.mean() >= 0.95
     with pytest.raises(ValueError, match="init_state batch size"):
         ik.solve(T, init_state=robot.state(first.q.numpy()[:8]))

@@ -39,9 +39,9 @@ def test_floating_base_solver_reaches_targets_beyond_the_fixed_arm(gpu, panda_ar
     ik = IKSolver(_config(), robot, "panda_hand")
     sol = ik.solve(T)
     assert sol.has_floating_base and sol.q.shape == (B, 7)
-    assert ik.compute_metrics(sol, T).success.mean() >= 0.9
+    assert ik.compute_metrics_numpy(sol, T).success.mean() >= 0.9
     fixed = IKSolver(presets.basic, robot, "panda_hand")
-    assert fixed.compute_metrics(fixed.solve(T), T).success.mean() < 0.9  # some targets out of a fixed arm's reach
+    assert fixed.compute_metrics_numpy(fixed.solve(T), T).success.mean() < 0.9  # some targets out of a fixed arm's reach
 
 
 def test_locked_base_and_joint_masks(gpu, panda_arm_spec):
@@ -54,7 +54,7 @@ def test_locked_base_and_joint_masks(gpu, panda_arm_spec):
     ik = IKSolver(_config(base_active_mask=(0.0, 0.0, 0.0, 0.0, 0.0, 0.0)), robot, "panda_hand")
     sol = ik.solve(T)
     np.testing.assert_array_equal(sol.T_world_base.numpy(), np.tile([0, 0, 0, 1, 0, 0, 0], (B, 1)))
-    assert ik.compute_metrics(sol, T).success.mean() >= 0.9
+    assert ik.compute_metrics_numpy(sol, T).success.mean() >= 0.9
     mask = np.ones(7, np.float32)
     mask[6] = 0.0
     ik.set_active_joint_mask(mask)
@@ -80,7 +80,7 @@ def test_floating_previous_and_rest_states(gpu, panda_arm_spec):
     cfg.add(ConfigurationTask(T_world_base_rest=IKContext.REST_BASE, include_joints=False, base_weight=1.0))
     ik = IKSolver(cfg, robot, "panda_hand")
     first = ik.solve(T)
-    assert ik.compute_metrics(first, T).success.mean() >= 0.8
+    assert ik.compute_metrics_numpy(first, T).success.mean() >= 0.8
     first_q, first_base = first.q.numpy().copy(), first.T_world_base.numpy().copy()  # solve reuses its buffers
     prev = robot.state(first_q, first_base)
     again = ik.solve(T, prev_state=prev)
@@ -89,7 +89,7 @@ def test_floating_previous_and_rest_states(gpu, panda_arm_spec):
         again.T_world_base.numpy() == prev.T_world_base.numpy(), axis=1)
     prev_cost, cost = ik._prev_cost.numpy(), ik.costs.numpy()
     assert (prev_cost[same] <= cost[same]).all() and (prev_cost[~same] > cost[~same]).all()
-    assert ik.compute_metrics(again, T).success.mean() >= 0.8
+    assert ik.compute_metrics_numpy(again, T).success.mean() >= 0.8
     rest = robot.state(first_q, np.tile([0.3, 0, 0, 1, 0, 0, 0], (B, 1)).astype(np.float32))
     moved = ik.solve(T, rest_state=rest)
     # the rest base pulls the base toward x = 0.3

@@ -162,7 +162,7 @@ def test_iksolver_keeps_a_previous_solution_that_scores_no_worse(gpu, panda_arm_
     moved = ik.solve(T, prev_state=robot.state(far)).q.numpy()
     assert np.abs(moved - far).max() > 1e-3
     # 30 iterations from the midrange with the pull toward a far previous state: most targets still reached
-    assert ik.compute_metrics(robot.state(moved), T).success.mean() >= 0.7
+    assert ik.compute_metrics_numpy(robot.state(moved), T).success.mean() >= 0.7
 
 
 def test_iksolver_smooth_preset_stays_near_the_previous_state(gpu, panda_arm_spec):
@@ -179,7 +179,7 @@ def test_iksolver_smooth_preset_stays_near_the_previous_state(gpu, panda_arm_spe
     plain = IKSolver(presets.basic, robot, "panda_hand")
     a = ik.solve(T, prev_state=robot.state(prev)).q.numpy()
     b = plain.solve(T).q.numpy()
-    assert ik.compute_metrics(robot.state(a), T).success.mean() >= 0.9
+    assert ik.compute_metrics_numpy(robot.state(a), T).success.mean() >= 0.9
     # the smoothness pull keeps the redundant arm near prev more often than an unregularised solve
     assert np.median(np.abs(a - prev).max(axis=1)) <= np.median(np.abs(b - prev).max(axis=1))
 

@@ -157,7 +157,7 @@ def test_iksolver_with_a_scene(gpu, panda_collision_spec):
                                margin=0.01, movable_only=True))
     ik = IKSolver(cfg, robot, "panda_hand", scene=scene)
     free = ik.solve(T).q.numpy().copy()  # scene indices default to 0: no slab
-    assert ik.compute_metrics(robot.state(free), T).success.mean() >= 0.9
+    assert ik.compute_metrics_numpy(robot.state(free), T).success.mean() >= 0.9
     blocked = ik.solve(T, scene_indices=np.ones(B, np.int32)).q.numpy()
     with pytest.raises(ValueError):
         ik.solve(T, scene_indices=np.ones(B // 2, np.int32))
