@@ -481,3 +481,128 @@ def test_keep_previous_prices_on_the_reference_scale(gpu, panda_arm_spec, preset
     np.testing.assert_allclose(pc, scale * np.sum(r ** 2, axis=1), rtol=1e-4, atol=2e-7)  # FP32 residuals
     kept = np.all(sol == prev_q, axis=1)
     np.testing.assert_array_equal(kept, pc <= cost)
+
+
+# --- heterogeneous scenes (test_ik.py:852-955, tests/helpers/motion_plan/hetero_scenes.py:1-100) -----------------
+# The reference's icosphere meshes are replaced by analytic spheres of the same radii.
+SCENE_IDS = [0, 0, 0, 1, 2, 2, 2, 2]
+SCENE_SPECS = [
+    {"boxes": [((0.05, 0.05, 0.3), (0.45, 0.16, 0.3)), ((0.05, 0.05, 0.3), (0.45, -0.16, 0.3))], "planes": [],
+     "spheres": []},
+    {"boxes": [((0.08, 0.35, 0.04), (0.45, 0.0, 0.25))], "planes": [], "spheres": [(0.11, (0.45, 0.0, 0.5))]},
+    {"boxes": [((0.05, 0.05, 0.25), (0.45, 0.0, 0.28))], "planes": [-0.05],
+     "spheres": [(0.1, (0.4, 0.22, 0.42)), (0.1, (0.4, -0.22, 0.42))]},
+]
+
+
+def _at(centers):
+    return [[*c, 1.0, 0.0, 0.0, 0.0] for c in centers]
+
+
+def _build_scene(ids):
+    """One Scene over the listed scene specs, one geometry per primitive type (empty types left out)."""
+    from robokit_b200.geom import BoxGeom, PlaneGeom, Scene, SphereGeom
+
+    specs = [SCENE_SPECS[i] for i in ids]
+    scene = Scene(len(specs))
+    he = [h for s in specs for h, _ in s["boxes"]]
+    off = np.cumsum([0] + [len(s["boxes"]) for s in specs])
+    scene.add(BoxGeom(he, off, poses=_at([c for s in specs for _, c in s["boxes"]])))
+    if any(s["planes"] for s in specs):
+        off = np.cumsum([0] + [len(s["planes"]) for s in specs])
+        scene.add(PlaneGeom(off, poses=_at([(0.0, 0.0, z) for s in specs for z in s["planes"]])))
+    if any(s["spheres"] for s in specs):
+        off = np.cumsum([0] + [len(s["spheres"]) for s in specs])
+        scene.add(SphereGeom([r for s in specs for r, _ in s["spheres"]], off,
+                             poses=_at([c for s in specs for _, c in s["spheres"]])))
+    return scene
+
+
+def _penetration(robot, scene, q):
+    """Deepest penetration of a collision sphere into the scene at each row of q (the "plain" penalty at
+    margin 0 is max(0, -signed distance))."""
+    from robokit_b200.opt import VarKey, VarValues
+    from robokit_b200.terms.dense import SceneCollisionTask
+
+    t = SceneCollisionTask(robot, scene, weight=1.0, margin=0.0, penalty="plain")
+    return t.compute_weighted_residual(VarValues({VarKey.ROBOT: robot.state(np.atleast_2d(q))})).numpy().max(axis=1)
+
+
+def _sample_targets(robot):
+    """A collision-free configuration per query in its own scene and its hand pose (hetero_scenes.py:113-133)."""
+    rng = np.random.default_rng(0)
+    lim = robot.spec.actuated_joint_limits
+    hand = robot.link_names.index(HAND)
+    start = np.tile(robot.spec.midrange_q.astype(np.float32), (len(SCENE_IDS), 1))
+    poses = []
+    for sid in SCENE_IDS:
+        scene = _build_scene([sid])
+        while True:
+            q = rng.uniform(lim[:, 0] * 0.6, lim[:, 1] * 0.6).astype(np.float32)
+            if _penetration(robot, scene, q)[0] == 0.0:
+                break
+        poses.append(robot.forward_kinematics(robot.state(q[None])).get_T_world_link(hand).numpy()[0])
+    return start, np.asarray(poses, np.float32)
+
+
+def _collision_config(robot, scene, scene_indices, solver, scale):
+    from robokit_b200.terms.dense import SceneCollisionTask
+
+    cfg = (IKSolverConfig(solver=solver, sampler=RobertsSamplerConfig(keep_first=True, scale=scale))
+           .add(PositionTask(frame_index=IKContext.TARGET_LINKS, T_world_target=IKContext.TARGET, weight=20.0))
+           .add(RotationTask(frame_index=IKContext.TARGET_LINKS, T_world_target=IKContext.TARGET, weight=10.0))
+           .add(PositionLimit(weight=50.0)))
+    for geometry in scene.geoms:
+        cfg.add(SceneCollisionTask(robot, scene=scene, geometry=geometry, scene_indices=scene_indices, weight=100.0,
+                                   margin=0.02))
+    return cfg
+
+
+def test_heterogeneous_collision_ik_matches_single_scenes(gpu, panda_collision_spec):
+    """TestHeterogeneousCollisionIK.test_matches_single_scene (test_ik.py:852-889): one candidate, batched over
+    three scenes, equals each query solved alone in its own scene."""
+    robot = _robot(panda_collision_spec)
+    start, T = _sample_targets(robot)
+    solver = PopulationSolverConfig(stages=[Stage(40, 1, LMOptimizerConfig(lm_lambda=1.0))], cuda_graph_mode="none")
+    idx = N.DeviceArray.from_numpy(np.asarray(SCENE_IDS, np.int32))
+    ik = IKSolver(_collision_config(robot, _build_scene([0, 1, 2]), idx, solver, 0.0), robot, HAND)
+    batched = ik.solve(T[:, None], init_state=robot.state(start), scene_indices=idx).q.numpy().copy()
+    for i, sid in enumerate(SCENE_IDS):
+        one = IKSolver(_collision_config(robot, _build_scene([sid]), None, solver, 0.0), robot, HAND)
+        qi = one.solve(T[i:i + 1, None], init_state=robot.state(start[i:i + 1])).q.numpy()
+        np.testing.assert_allclose(batched[i], qi[0], atol=1e-4, err_msg=f"query {i} (scene {sid})")
+
+
+def test_heterogeneous_collision_ik_is_collision_free(gpu, panda_collision_spec):
+    """TestHeterogeneousCollisionIK.test_collision_free_per_scene (test_ik.py:924-955)."""
+    robot = _robot(panda_collision_spec)
+    start, T = _sample_targets(robot)
+    idx = N.DeviceArray.from_numpy(np.asarray(SCENE_IDS, np.int32))
+    ik = IKSolver(_collision_config(robot, _build_scene([0, 1, 2]), idx, presets.smooth.solver, 1.0), robot, HAND)
+    q = ik.solve(T[:, None], init_state=robot.state(start), scene_indices=idx).q.numpy().copy()
+    (pos, _), = _errors(robot, robot.state(q), [HAND], T)
+    for i, sid in enumerate(SCENE_IDS):
+        assert _penetration(robot, _build_scene([sid]), q[i])[0] <= 0.001, f"query {i} collides in scene {sid}"
+        assert pos[i] < 0.02, f"query {i} missed its target by {pos[i] * 1000:.1f} mm"
+
+
+@pytest.mark.parametrize("mode", ["none", "iter", "full"])
+def test_prev_state_with_scene_collision(gpu, panda_collision_spec, mode):
+    """TestIKPreviousStateWithSceneCollision (test_ik.py:958-986): pricing prev_state (one row per target) before
+    the multi-candidate solve leaves the candidates' collision term intact."""
+    from robokit_b200.geom import Scene, SphereGeom
+    from robokit_b200.terms.dense import SceneCollisionTask
+
+    robot = _robot(panda_collision_spec)
+    scene = Scene(1).add(SphereGeom([0.05], [0, 1], poses=[[2.0, 2.0, 2.0, 1.0, 0.0, 0.0, 0.0]]))
+    cfg = IKSolverConfig()
+    cfg.solver = PopulationSolverConfig(stages=cfg.solver.stages, cuda_graph_mode=mode)
+    cfg = (cfg.add(PositionTask(frame_index=IKContext.TARGET_LINKS, T_world_target=IKContext.TARGET, weight=20.0))
+           .add(RotationTask(frame_index=IKContext.TARGET_LINKS, T_world_target=IKContext.TARGET, weight=10.0))
+           .add(SceneCollisionTask(scene=IKContext.SCENE, scene_indices=IKContext.SCENE_INDICES, weight=100.0)))
+    ik = IKSolver(cfg, robot, HAND, scene=scene)
+    q = robot.spec.midrange_q.astype(np.float32)[None]
+    state = robot.state(q)
+    pose = robot.forward_kinematics(robot.state(q)).get_T_world_link(robot.link_names.index(HAND)).numpy()
+    solved = ik.solve(pose[:, None], prev_state=state, init_state=state).q.numpy()
+    np.testing.assert_allclose(solved, q, atol=1e-4)
