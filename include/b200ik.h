@@ -353,6 +353,12 @@ int ik_integrate(int32_t batch, int32_t num_actuated, int32_t floating_base, con
 int ik_copy_rows(int32_t rows, int32_t width, const float* d_src, int64_t src_stride, float* d_dst, int64_t dst_stride,
                  void* stream);
 
+/* Row gather, RobotState.gather (robo/robot_state.py:478-520): d_dst[r*width + c] =
+ * d_src[d_index[r]*width + c].  An index outside [0, src_rows) leaves its row
+ * unwritten and adds one to *d_bad (when d_bad is not NULL). */
+int ik_gather_rows(int32_t rows, int32_t width, const int32_t* d_index, int32_t src_rows, const float* d_src,
+                   float* d_dst, int32_t* d_bad, void* stream);
+
 /* Masked row copy, RobotState.accept (robo/robot_state.py:448-476,
  * robot_kernels.py:744-767): rows with d_mask[r] == 1 copy `width` floats. */
 int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, const float* d_src, float* d_dst,

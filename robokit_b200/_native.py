@@ -209,6 +209,7 @@ _SIGNATURES = {
     "ik_row_sumsq": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64, _vp, ctypes.c_int32, _vp]),
     "ik_pose_from_matrix": (ctypes.c_int, [ctypes.c_int32, _vp, _vp, _vp]),
     "ik_matrix_from_pose": (ctypes.c_int, [ctypes.c_int32, _vp, _vp, _vp]),
+    "ik_gather_rows": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp]),
     "ik_copy_rows": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp]),
     "ik_masked_copy_rows": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, _vp, _vp, _vp]),
     "ik_select_best": (

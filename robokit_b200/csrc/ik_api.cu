@@ -1448,6 +1448,16 @@ int ik_copy_rows(int32_t rows, int32_t width, const float* d_src, int64_t src_st
     return check_launch();
 }
 
+int ik_gather_rows(int32_t rows, int32_t width, const int32_t* d_index, int32_t src_rows, const float* d_src,
+                   float* d_dst, int32_t* d_bad, void* stream) {
+    if (rows < 0 || width < 0 || src_rows < 0) return fail(IK_E_INVALID, "negative size");
+    if (rows == 0 || width == 0) return IK_OK;
+    if (!d_index || !d_src || !d_dst) return fail(IK_E_INVALID, "NULL array");
+    gather_rows_kernel<<<elementwise_grid((long long)rows * width), 256, 0, S(stream)>>>(rows, width, d_index,
+                                                                                         src_rows, d_src, d_dst, d_bad);
+    return check_launch();
+}
+
 int ik_masked_copy_rows(int32_t rows, int32_t width, const int32_t* d_mask, const float* d_src, float* d_dst,
                         void* stream) {
     if (rows < 0 || width < 0) return fail(IK_E_INVALID, "negative size");

@@ -534,6 +534,22 @@ __global__ void copy_rows_kernel(int rows, int width, const float* src, long lon
     }
 }
 
+// Row gather: dst[r, :] = src[index[r], :].  An index outside [0, src_rows) leaves its row untouched and is
+// counted in *bad (robo/robot_state.py gather, robot_kernels.py gather kernels).
+__global__ void gather_rows_kernel(int rows, int width, const int* index, int src_rows, const float* src, float* dst,
+                                   int* bad) {
+    const long long n = (long long)rows * width;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / width, c = i - r * width;
+        const int s = index[r];
+        if (s < 0 || s >= src_rows) {
+            if (c == 0 && bad) atomicAdd(bad, 1);
+            continue;
+        }
+        dst[i] = src[(long long)s * width + c];
+    }
+}
+
 __global__ void masked_copy_rows_kernel(int rows, int width, const int* mask, const float* src, float* dst) {
     const long long n = (long long)rows * width;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {

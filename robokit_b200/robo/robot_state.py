@@ -52,6 +52,12 @@ class RobotState(Var):
 
     # --- lazily allocated derived buffers ------------------------------------------
     def __getattr__(self, name: str):
+        if name in _LAZY and "_view_source" in self.__dict__:
+            # a view's buffers are rows of its source's (allocated there on first use)
+            off = self.__dict__["_view_offset"]
+            arr = getattr(self.__dict__["_view_source"], name).row_slice(off, off + self.batch_size)
+            self.__dict__[name] = arr
+            return arr
         if name in _LAZY:
             B, s = self.batch_size, self.spec
             ns = len(s.collision_sphere_radii)
@@ -187,22 +193,70 @@ class RobotState(Var):
         self.is_collision_spheres_computed = False
         return self
 
+    def _copy_flags(self, st: "RobotState") -> None:
+        st.has_floating_base = self.has_floating_base
+        st.is_fk_computed = self.is_fk_computed
+        st.is_motion_subspace_computed = self.is_motion_subspace_computed
+        st.is_collision_spheres_computed = self.is_collision_spheres_computed
+        st.base_step_scale, st.clamp_q_on_integrate = self.base_step_scale, self.clamp_q_on_integrate
+
     def clone(self) -> "RobotState":
-        return RobotState(self.robot, self.q.clone(), self.T_world_base.clone() if self.has_floating_base else None)
+        """Copies of q, the base and every derived buffer already allocated, with the same computed flags
+        (robo/robot_state.py:335-354)."""
+        st = RobotState.__new__(RobotState)
+        st.robot, st.spec = self.robot, self.spec
+        st.q, st.T_world_base = self.q.clone(), self.T_world_base.clone()
+        for name in _LAZY:
+            if name in self.__dict__:
+                st.__dict__[name] = self.__dict__[name].clone()
+        self._copy_flags(st)
+        return st
 
     def view(self, batch_size: int, offset: int = 0) -> "RobotState":
-        """Rows [offset, offset+batch_size) sharing storage."""
+        """Rows [offset, offset+batch_size) of every buffer, sharing storage and the computed flags
+        (robo/robot_state.py:356-380)."""
+        if offset < 0 or batch_size < 0 or offset + batch_size > self.batch_size:
+            raise ValueError(f"view [{offset}, {offset + batch_size}) outside a batch of {self.batch_size}")
         st = RobotState.__new__(RobotState)
         st.robot, st.spec = self.robot, self.spec
         st.q = self.q.row_slice(offset, offset + batch_size)
         st.T_world_base = self.T_world_base.row_slice(offset, offset + batch_size)
-        st.has_floating_base = self.has_floating_base
-        st.base_step_scale, st.clamp_q_on_integrate = self.base_step_scale, self.clamp_q_on_integrate
-        st.invalidate()
+        st.__dict__["_view_source"], st.__dict__["_view_offset"] = self, offset
+        for name in _LAZY:
+            if name in self.__dict__:
+                st.__dict__[name] = self.__dict__[name].row_slice(offset, offset + batch_size)
+        self._copy_flags(st)
         return st
 
-    def gather(self, indices: Any, out: Optional["RobotState"] = None) -> "RobotState":
-        idx = np.asarray(indices.numpy() if hasattr(indices, "numpy") else indices, np.int64)
-        q = self.q.numpy()[idx]
-        base = self.T_world_base.numpy()[idx] if self.has_floating_base else None
-        return RobotState(self.robot, q, base)
+    def gather(self, indices: Any, out: Optional["RobotState"] = None, q_only: bool = True) -> "RobotState":
+        """Rows `indices` of q and the base into `out` (allocated when omitted); with q_only=False also the
+        base of a fixed-base state, the link and joint poses and every other derived buffer already
+        allocated, with the source's computed flags (robo/robot_state.py:410-446).  Device gathers; an
+        index outside the batch raises IndexError."""
+        idx = N.as_device(indices, np.int32)
+        n = idx.shape[0]
+        if out is None:
+            out = RobotState(self.robot, N.DeviceArray.empty((n, self.spec.num_actuated_joints)),
+                             N.DeviceArray.empty((n, 7)) if self.has_floating_base else None)
+        elif out.batch_size != n:
+            raise ValueError(f"out holds {out.batch_size} rows, {n} indices given")
+        bad = N.DeviceArray.zeros(1, np.int32)
+        src_rows = self.batch_size
+
+        def rows(src: N.DeviceArray, dst: N.DeviceArray) -> None:
+            width = int(np.prod(src.shape[1:]))
+            N.check(N.lib().ik_gather_rows(n, width, idx.ptr, src_rows, src.ptr, dst.ptr, bad.ptr, None))
+
+        rows(self.q, out.q)
+        if self.has_floating_base or not q_only:
+            rows(self.T_world_base, out.T_world_base)
+        if not q_only:
+            for name in _LAZY:
+                if name in ("T_world_joint", "T_world_link") or name in self.__dict__:
+                    rows(getattr(self, name), getattr(out, name))
+        if int(bad.numpy()[0]):
+            raise IndexError(f"gather index outside a batch of {src_rows}")
+        self._copy_flags(out)
+        if q_only:
+            out.is_fk_computed = out.is_motion_subspace_computed = out.is_collision_spheres_computed = False
+        return out
