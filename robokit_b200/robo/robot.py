@@ -134,8 +134,12 @@ class Robot:
             return state
         return self.forward_kinematics(state)
 
-    def sample_q(self, batch_size: int, seed: Optional[int] = None) -> np.ndarray:
-        """Uniform joint positions within the limits (robo/robot.py:633)."""
-        rng = np.random.default_rng(seed)
+    def sample_q(self, num_samples: int = 1, rng: Optional[np.random.Generator] = None, device: Any = None,
+                 seed: Optional[int] = None) -> np.ndarray:
+        """`num_samples` joint configurations, uniform within the limits, as a host float32 array
+        (robo/robot.py:633-650); `rng` (a numpy Generator) or `seed` picks the stream."""
+        if device is not None and not str(device).startswith("cuda"):
+            raise ValueError(f"device {device!r}: this library runs on CUDA only (no CPU fallback)")
+        rng = rng if rng is not None else np.random.default_rng(seed)
         lim = self.spec.float32_actuated_limits()
-        return rng.uniform(lim[:, 0], lim[:, 1], size=(batch_size, lim.shape[0])).astype(np.float32)
+        return rng.uniform(lim[:, 0], lim[:, 1], size=(num_samples, lim.shape[0])).astype(np.float32)

@@ -65,7 +65,7 @@ class RobotState(Var):
                 "T_world_joint": (B, s.num_joints, 7),
                 "T_world_link": (B, s.num_links, 7),
                 "S_world": (B, 6, max(s.num_joints, 1)),
-                "collision_sphere_centers_world": (B, max(ns, 1), 3),
+                "collision_sphere_centers_world": (B, ns, 3),
                 "link_bounding_sphere_centers_world": (B, s.num_links, 3),
             }
             arr = N.DeviceArray.zeros(shapes[name], np.float32)
