@@ -88,6 +88,7 @@ class IKSolver:
                     raise ValueError(f"link index {x} out of range [0, {len(names)})")
                 self.target_links.append(int(x))
         self.num_targets = len(self.target_links)
+        self.target_link_indices = self.target_links  # the reference's attribute name
         for t in (*config.terms, *config.score_terms):  # a term on the target links may weigh each link
             w = getattr(t, "weight", None)
             if isinstance(w, (list, tuple)) and _on_target_links(t) and len(w) != self.num_targets:
@@ -464,7 +465,7 @@ class IKSolver:
     def solve(self, T_world_target: Any, prev_state: Optional[RobotState] = None,
               init_state: Optional[RobotState] = None, rest_state: Optional[RobotState] = None,
               out_state: Optional[RobotState] = None, init_sample_range: Optional[float] = None,
-              scene_indices: Any = None, base_init_sample_range: Optional[Sequence[float]] = None) -> RobotState:
+              base_init_sample_range: Optional[Sequence[float]] = None, scene_indices: Any = None) -> RobotState:
         """Solutions for every target, instance-major: (batch * num_solutions, dofs) (helpers/ik/ik.py:223-304).
 
         prev_state (batch,) fills IKContext.PREVIOUS_STATE and is kept for a target where it costs no more
