@@ -163,3 +163,45 @@ def test_fk_on_a_view_writes_the_source_rows(gpu, robot):
     zero = robot.forward_kinematics(robot.state(np.zeros((1, na), np.float32))).T_world_link.numpy()[0]
     np.testing.assert_array_equal(got[0], zero)
     np.testing.assert_array_equal(got[3], zero)
+
+
+def _frees_without_gc(build):
+    """tests/test_frees_without_gc.py:24-29: the object dies by refcount alone, with the collector off."""
+    import gc
+    import weakref
+
+    gc.disable()
+    try:
+        ref = weakref.ref(build())
+        return ref() is None
+    finally:
+        gc.enable()
+
+
+def test_solved_optimizer_and_ik_solver_free_without_gc(gpu, panda_arm_spec):
+    """A solved LMOptimizer and an IKSolver that captured its solve graph hold no reference cycles, so their device
+    buffers, problems and graphs are released as soon as the last reference goes."""
+    from robokit_b200.helpers.ik import IKSolver, presets
+    from robokit_b200.opt import LMOptimizer, LMOptimizerConfig, VarKey, VarValues
+    from robokit_b200.robo.robot import Robot
+    from robokit_b200.terms.dense import PositionLimit, PositionTask
+
+    robot = Robot(panda_arm_spec)
+    hand = robot.link_names.index("panda_hand")
+    q = robot.sample_q(8, seed=1)
+    T = robot.forward_kinematics(robot.state(q)).get_T_world_link(hand).numpy().reshape(8, 1, 7)
+
+    def optimizer():
+        opt = LMOptimizer([PositionTask(robot, hand, T, weight=1.0), PositionLimit(robot, weight=1.0)],
+                          LMOptimizerConfig(max_iter=5))
+        opt.solve(VarValues({VarKey.ROBOT: robot.state(np.zeros_like(q))}))
+        return opt
+
+    def solver():
+        ik = IKSolver(presets.basic, robot, "panda_hand")
+        ik.solve(T)
+        ik.solve(T)  # the second solve replays the captured graph
+        return ik
+
+    assert _frees_without_gc(optimizer)
+    assert _frees_without_gc(solver)
