@@ -2,6 +2,6 @@
 
 from . import presets
 from .config import IKContext, IKSolverConfig
-from .ik import IKMetrics, IKSolver
+from .ik import IKMetrics, IKResultTorch, IKSolver
 
-__all__ = ["IKContext", "IKMetrics", "IKSolver", "IKSolverConfig", "presets"]
+__all__ = ["IKContext", "IKMetrics", "IKResultTorch", "IKSolver", "IKSolverConfig", "presets"]

@@ -26,18 +26,18 @@ and its solutions come back sorted best first (opt/population_solver.py:163-202,
 from __future__ import annotations
 
 import ctypes
-from dataclasses import replace
-from typing import Any, Dict, List, NamedTuple, Optional, Sequence, Union
+from typing import Any, Dict, NamedTuple, Optional, Sequence, Union
 
 import numpy as np
 
 from ... import _native as N
 from ...opt.lm_optimizer import LMOptimizer, LMOptimizerConfig
+from ...opt.population_solver import build_stages, run_stages
 from ...opt.sampler import RobertsSampler
 from ...opt.var_values import VarKey, VarValues
 from ...robo.robot_state import RobotState
-from ...terms.dense import (ConfigurationTask, FrameTask, PositionLimit, PositionTask, RotationTask,
-                            SceneCollisionTask, SelfCollisionTask, SmoothnessTask, VelocityLimitTask, _PoseTask)
+from ...terms.dense import (ConfigurationTask, FrameTask, PositionLimit, SceneCollisionTask, SelfCollisionTask,
+                            SmoothnessTask, VelocityLimitTask, _PoseTask)
 from ...terms.task import Context
 from .config import IKContext, IKSolverConfig
 
@@ -151,12 +151,11 @@ class IKSolver:
 
     def _relower(self) -> None:
         """Lower every problem whose terms changed again (same capacity) and drop the captured graph."""
-        for _, _, state, opt in self._stages:
-            if opt is not None:
-                opt.reset(VarValues({VarKey.ROBOT: state}))
-        for r in self._rankers:
-            if r is not None:
-                r[0].reset(VarValues({VarKey.ROBOT: r[1]}))
+        for st in self._stages:
+            if st.opt is not None:
+                st.opt.reset(VarValues({VarKey.ROBOT: st.state}))
+            if st.ranker is not None:
+                st.ranker[0].reset(VarValues({VarKey.ROBOT: st.ranker[1]}))
         if self._scorer is not None:
             self._scorer.reset(VarValues({VarKey.ROBOT: self._prev_save}))
         self._cost_groups = None
@@ -275,17 +274,10 @@ class IKSolver:
         self._pose_terms = [t for t in (*self._terms, *self._score_terms) if isinstance(t, _PoseTask)]
         for t in self._pose_terms:  # every stage's problem (and every score problem) reads the one target buffer
             t.bind_targets(self._targets)
-        self._stages = []
         self._mask = self._dof_mask()
-        for k, (width, lm) in enumerate(zip(self.widths, self.lm_configs)):
-            iters = self.config.solver.stages[k].iters
-            state = self._state(B * width)
-            opt = None
-            if iters > 0:
-                cfg = replace(lm, max_iter=iters, early_stopping_interval=0, form="persistent")
-                opt = LMOptimizer(self._terms, cfg, active_dof_mask=self._mask)
-                opt.reset(VarValues({VarKey.ROBOT: state}))
-            self._stages.append((width, iters, state, opt))
+        # LM problem per stage, score problems where score terms rank (opt/population_solver.py:179-270)
+        self._stages = build_stages(self.robot, self.floating, B, self.config.solver, self._terms, self._score_terms,
+                                    self._mask)
         C0 = self.widths[0]
         lim = spec.float32_actuated_limits()
         self._range = (lim[:, 1] - lim[:, 0]).astype(np.float32)
@@ -300,24 +292,9 @@ class IKSolver:
         self._noise_mid = N.DeviceArray.from_numpy(self._sampler.tangent(B, self._tangent_scale(1.0, None)))
         self._noise_scale = None
         self._noise = None
-        self._cost = [N.DeviceArray.zeros(B * w) for w in self.widths]
-        self._params = [None if opt is None else opt.config.native_params() for (_, _, _, opt) in self._stages]
         self._stream = N.Stream()
         self._graph: Optional[N.Graph] = None
         self._scorer: Optional[LMOptimizer] = None  # prices a previous state (built on the first one)
-        # score terms: a zero-iteration problem over them per ranked stage, with a scratch copy of the candidates
-        # (all stages, or with rank_final only the last: opt/population_solver.py:179-186)
-        self._rankers: List[Optional[tuple]] = []
-        last = len(self._stages) - 1
-        for k, (width, _, _, _) in enumerate(self._stages):
-            if self._score_terms and (not self.config.solver.rank_final or k == last):
-                scratch = self._state(B * width)
-                sc = LMOptimizer(self._score_terms, LMOptimizerConfig(max_iter=0, form="persistent"),
-                                 active_dof_mask=self._mask)
-                sc.reset(VarValues({VarKey.ROBOT: scratch}))
-                self._rankers.append((sc, scratch, sc.config.native_params()))
-            else:
-                self._rankers.append(None)
         self._ranked = None
         if self.config.solver.rank_final and self.num_solutions > 1:  # final rows sorted best first
             self._ranked = self._state(B * self.num_solutions)
@@ -353,7 +330,7 @@ class IKSolver:
             N.check(N.lib().ik_memcpy_dtod(self._prev_save.T_world_base.ptr, src.ptr, src.nbytes, stream))
         sc = self._scorer
         sc._slice(B)
-        if self._stages[-1][1] > 0 and self._rankers[-1] is None:
+        if self._stages[-1].iters > 0 and self._stages[-1].ranker is None:
             # The solve ends on LM iterations and reports the optimizer's 0.5 |r|^2, which the reference compares
             # with prev_state's |r|^2 (helpers/ik/ik.py:257-289, opt/population_solver.py:427-428): price prev
             # the same way.  After a select stage or with score terms both sides share one scale.
@@ -382,7 +359,7 @@ class IKSolver:
         """Candidates spread around init_state's joints and base (helpers/ik/ik.py:486-540)."""
         B, C0 = self._batch, self.widths[0]
         na = self.num_joints
-        state = self._stages[0][2]
+        state = self._stages[0].state
         if init_state.batch_size != B:
             raise ValueError(f"init_state batch size {init_state.batch_size} != {B}")
         rep = np.repeat(np.arange(B, dtype=np.int32), C0)
@@ -410,57 +387,16 @@ class IKSolver:
     def _device_body(self, stream: int) -> None:
         """Seed from the midrange, run every stage, select between stages: device work only, on `stream`."""
         B, C0, na = self._batch, self.widths[0], self.num_joints
-        q0 = self._stages[0][2]
+        q0 = self._stages[0].state
         N.check(N.lib().ik_integrate(B * C0, na, int(self.floating), self._mid.ptr, N.ptr(self._base0),
                                      self._noise_mid.ptr, None, q0.q.ptr,
                                      q0.T_world_base.ptr if self.floating else None, stream))
         N.check(N.lib().ik_clamp_q(B * C0, na, q0.q.ptr, self.robot.limits_device().ptr, None, stream))
         self._run_stages(stream)
 
-    def _rank_stage(self, k: int, stream: int) -> None:
-        """Price stage k's candidates with the score terms into its cost buffer (the select reads it)."""
-        sc, scratch, prm = self._rankers[k]
-        width, _, state, _ = self._stages[k]
-        n = self._batch * width
-        N.check(N.lib().ik_memcpy_dtod(scratch.q.ptr, state.q.ptr, n * self.num_joints * 4, stream))
-        if self.floating:
-            N.check(N.lib().ik_memcpy_dtod(scratch.T_world_base.ptr, state.T_world_base.ptr, n * 28, stream))
-        sc._slice(n)
-        N.check(N.lib().ik_solve_persistent(sc.problem.handle, n, scratch.q.ptr,
-                                            scratch.T_world_base.ptr if self.floating else None, ctypes.byref(prm),
-                                            self._cost[k].ptr, sc.lm.ptr, sc.iterations.ptr, sc.status.ptr, stream))
-
     def _run_stages(self, stream: int) -> None:
-        B, na = self._batch, self.num_joints
-        for k, (width, iters, state, opt) in enumerate(self._stages):
-            if opt is not None:
-                n = B * width
-                opt._slice(n)
-                N.check(N.lib().ik_solve_persistent(opt.problem.handle, n, state.q.ptr,
-                                                    state.T_world_base.ptr if self.floating else None,
-                                                    ctypes.byref(self._params[k]), self._cost[k].ptr, opt.lm.ptr,
-                                                    opt.iterations.ptr, opt.status.ptr, stream))
-            elif k == 0 and self._rankers[0] is None:
-                raise NotImplementedError("a first stage without iterations needs a scoring pass")
-            if self._rankers[k] is not None and (opt is not None or k == 0 or self._rankers[k - 1] is None):
-                self._rank_stage(k, stream)  # a select from a ranked stage already carries its scores
-            if k + 1 < len(self._stages):
-                nxt_w, _, nxt_state, _ = self._stages[k + 1]
-                fb = self.floating
-                N.check(N.lib().ik_select_best(B, width, nxt_w, self._cost[k].ptr, state.q.ptr,
-                                               state.T_world_base.ptr if fb else None, na, nxt_state.q.ptr,
-                                               nxt_state.T_world_base.ptr if fb else None, self._cost[k + 1].ptr,
-                                               None, stream))
-        if self._ranked is not None:
-            width, _, state, _ = self._stages[-1]
-            fb = self.floating
-            N.check(N.lib().ik_select_best(B, width, width, self._cost[-1].ptr, state.q.ptr,
-                                           state.T_world_base.ptr if fb else None, na, self._ranked.q.ptr,
-                                           self._ranked.T_world_base.ptr if fb else None, self._ranked_cost.ptr,
-                                           None, stream))
-            self._ranked.invalidate()
-        for _, _, state, _ in self._stages:
-            state.invalidate()
+        run_stages(self._stages, self._batch, self.floating, stream, self._ranked,
+                   self._ranked_cost if self._ranked is not None else None)
 
     def solve(self, T_world_target: Any, prev_state: Optional[RobotState] = None,
               init_state: Optional[RobotState] = None, rest_state: Optional[RobotState] = None,
@@ -493,10 +429,10 @@ class IKSolver:
                 self._graph.launch()
         else:
             self._device_body(st)
-        final = self._stages[-1][2]
+        final = self._stages[-1].state
         if prev_state is not None:
             fb = self.floating
-            N.check(N.lib().ik_keep_previous(B, self.num_joints, self._prev_cost.ptr, self._cost[-1].ptr,
+            N.check(N.lib().ik_keep_previous(B, self.num_joints, self._prev_cost.ptr, self._stages[-1].cost.ptr,
                                              self._prev_save.q.ptr, self._prev_save.T_world_base.ptr if fb else None,
                                              final.q.ptr, final.T_world_base.ptr if fb else None, st))
         N.check(N.lib().ik_stream_synchronize(st))
@@ -586,7 +522,7 @@ class IKSolver:
     def costs(self) -> N.DeviceArray:
         """Cost of each returned solution: 0.5 |r|^2 of the final stage's optimization terms, or of the score
         terms where they rank the final stage."""
-        return self._cost[-1] if self._ranked is None else self._ranked_cost
+        return self._stages[-1].cost if self._ranked is None else self._ranked_cost
 
     def compute_costs(self, state: RobotState, T_world_target: Any, prev_state: Optional[RobotState] = None,
                       scene_indices: Any = None) -> Dict[str, N.DeviceArray]:
