@@ -92,3 +92,23 @@ def test_population_solver_rejects_a_ragged_batch(gpu, panda_arm_spec):
         solver.solve(VarValues({VarKey.ROBOT: robot.state(q0[:C * B - 1])}))
     with pytest.raises(ValueError, match="CUDA only"):
         PopulationSolver(terms, PopulationSolverConfig(), device="cpu")
+
+
+def test_replay_solves_each_new_population(gpu, panda_arm_spec):
+    """TestCpuReplay.test_replay_solves_each_new_population (tests/opt/test_population_solver.py:266-285) on the
+    GPU: under "full" the recorded solve reads the population's buffers at replay, so new values written into
+    the same var give that population's solution; a new var is recorded again."""
+    robot, terms, q0 = _setup(panda_arm_spec, seed=7)
+    stages = [Stage(3, C, LMOptimizerConfig(lm_lambda=10.0)), Stage(2, 1)]
+    solver = PopulationSolver(terms, PopulationSolverConfig(stages=stages, cuda_graph_mode="full"))
+    var = VarValues({VarKey.ROBOT: robot.state(q0)})
+    solver.solve(var)
+    q_new = robot.sample_q(B * C, seed=99)
+    var.get(VarKey.ROBOT).q.assign(q_new)
+    replayed = solver.solve(var)[0].get(VarKey.ROBOT).q.numpy().copy()
+    fresh = PopulationSolver(terms, PopulationSolverConfig(stages=stages, cuda_graph_mode="none"))
+    want = fresh.solve(VarValues({VarKey.ROBOT: robot.state(q_new)}))[0].get(VarKey.ROBOT).q.numpy()
+    np.testing.assert_array_equal(replayed, want)
+    other = solver.solve(VarValues({VarKey.ROBOT: robot.state(q0)}))[0].get(VarKey.ROBOT).q.numpy().copy()
+    first = fresh.solve(VarValues({VarKey.ROBOT: robot.state(q0)}))[0].get(VarKey.ROBOT).q.numpy()
+    np.testing.assert_array_equal(other, first)
