@@ -61,7 +61,7 @@ class IKServer:
         """Register robot + terms + LM parameters; `slots` problems of this type may be in flight at once."""
         keep: List[Any] = []
         descs, ndesc = lower_terms(robot, list(terms), 1, floating, keep)
-        pose_frames = [int(descs[i].num_frames) for i in range(len(terms))
+        pose_frames = [int(descs[i].num_frames) for i in range(ndesc)
                        if descs[i].kind in (N.IK_TERM_POSITION, N.IK_TERM_ROTATION, N.IK_TERM_FRAME)]
         mask = None
         if active_dof_mask is not None:

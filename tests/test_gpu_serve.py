@@ -106,3 +106,30 @@ def test_server_errors(gpu):
         small.add_type(types[0].cfg.robot, types[0].cfg.terms, types[0].lm, 4096)
     small.close()
     srv.close()
+
+
+def test_server_refuses_terms_with_per_problem_references(gpu, panda_collision_spec):
+    """A request carries only seeds and pose targets: joint-reference, velocity, scene and base-reference terms
+    are refused when the type is registered."""
+    from robokit_b200.geom import BoxGeom, Scene
+    from robokit_b200.opt import LMOptimizerConfig
+    from robokit_b200.robo.robot import Robot
+    from robokit_b200.terms.dense import (ConfigurationTask, PositionTask, SceneCollisionTask, SmoothnessTask,
+                                          VelocityLimitTask)
+
+    robot = Robot(panda_collision_spec)
+    hand = robot.link_names.index("panda_hand")
+    pose = PositionTask(robot, hand, np.tile(np.array([0.4, 0, 0.4, 1, 0, 0, 0], np.float32), (1, 1, 1)))
+    prev = robot.state(panda_collision_spec.zero_q[None].astype(np.float32))
+    others = [SmoothnessTask(robot=robot, prev_var=prev, weight=1.0),
+              ConfigurationTask(robot=robot, rest_q=panda_collision_spec.zero_q.astype(np.float32), weight=1.0),
+              VelocityLimitTask(robot=robot, dt=0.1, prev_state_var=prev, weight=1.0),
+              SceneCollisionTask(robot, Scene(1).add(BoxGeom([[0.1, 0.1, 0.1]], [0, 1])), weight=1.0)]
+    srv = serve.IKServer(budget_bytes=64 << 20)
+    try:
+        for t in others:
+            with pytest.raises(N.NativeError, match="not served"):
+                srv.add_type(robot, [pose, t], LMOptimizerConfig(max_iter=5, early_stopping_interval=0), 16)
+        assert srv.add_type(robot, [pose], LMOptimizerConfig(max_iter=5, early_stopping_interval=0), 16) == 0
+    finally:
+        srv.close()
