@@ -272,7 +272,10 @@ int ik_server_destroy(IkServer* server);
 /* Register a problem type: robot + terms as for ik_problem_create, LM
  * parameters, and `slots` = problems of this type that may be admitted at
  * once.  The d_targets of pose terms are ignored: each request brings its
- * own targets.  IK_E_OOM when the slots do not fit the budget. */
+ * own targets.  Joint-reference, velocity-limit and base-reference terms must
+ * have target_rows == 1 (one reference shared by every problem, read in place),
+ * scene terms scene_rows <= 1; others fail with IK_E_UNSUPPORTED.  IK_E_OOM
+ * when the slots do not fit the budget. */
 int ik_server_add_type(IkServer* server, IkRobot* robot, int32_t floating_base, const IkTermDesc* terms,
                        int32_t num_terms, const float* active_dof_mask, const IkLmParams* params, int32_t slots,
                        int32_t* type_id);

@@ -42,8 +42,10 @@ __device__ __forceinline__ void load_point(const Group<G>& g, const Tabs& t, Ws&
     if (h->base_off && g.lane < 7) w.base[g.lane] = base[(size_t)p * 7 + g.lane];
 }
 
+// The references of problem p other than its pose targets: base reference poses, scene indices and joint
+// references, each read at the broadcast row of p (row p / (batch / rows)).
 template <int G>
-__device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
+__device__ __forceinline__ void load_refs(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
     const TabHeader* h = t.h;
     for (int it = g.lane; it < h->nbref * 7; it += G) {
         const BaseRefEntry& be = t.bref()[it / 7];
@@ -74,6 +76,12 @@ __device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, W
         float* dst = reinterpret_cast<float*>(w.raw) + jr.ws_ref;
         for (int a = g.lane; a < h->na; a += G) dst[a] = jr.ref[(size_t)row * h->na + a];
     }
+}
+
+template <int G>
+__device__ __forceinline__ void load_targets(const Group<G>& g, const Tabs& t, Ws& w, int p, int batch) {
+    const TabHeader* h = t.h;
+    load_refs<G>(g, t, w, p, batch);
     const int items = h->npose * 7;
     for (int it = g.lane; it < items; it += G) {
         const int e = it / 7, c = it - 7 * e;

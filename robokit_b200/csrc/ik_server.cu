@@ -109,6 +109,8 @@ __device__ __forceinline__ void load_request_point(const Group<G>& g, const Tabs
         const PoseEntry& pe = t.pose()[e];
         w.tgt()[8 * e + k] = __ldcv(pe.targets + ((size_t)slot * pe.num_frames + pe.frame) * 7 + k);
     }
+    // the type's shared references: one row per joint or base reference, one scene (checked at registration)
+    load_refs<G>(g, t, w, 0, 1);
 }
 
 template <int G>
@@ -569,11 +571,15 @@ int ik_server_add_type(IkServer* S, IkRobot* robot, int32_t floating_base, const
     T->slots = slots;
     T->params = *params;
     for (int i = 0; i < num_terms; ++i)
-        if (descs[i].kind == IK_TERM_JOINT_REF || descs[i].kind == IK_TERM_VELOCITY_LIMIT ||
-            descs[i].kind == IK_TERM_SCENE_COLLISION || descs[i].kind == IK_TERM_BASE_REF) {
+        if ((descs[i].kind == IK_TERM_JOINT_REF || descs[i].kind == IK_TERM_VELOCITY_LIMIT ||
+             descs[i].kind == IK_TERM_BASE_REF) && descs[i].target_rows != 1) {
             delete T;
-            return fail(IK_E_UNSUPPORTED, "term %d: joint-reference and scene terms are not served (no per-request "
-                        "references or scenes)", i);
+            return fail(IK_E_UNSUPPORTED, "term %d: a served reference term needs one shared reference row, not %d "
+                        "(requests carry no references)", i, descs[i].target_rows);
+        } else if (descs[i].kind == IK_TERM_SCENE_COLLISION && descs[i].scene_rows > 1) {
+            delete T;
+            return fail(IK_E_UNSUPPORTED, "term %d: a served scene term needs one scene for every problem, not %d "
+                        "scene rows (requests carry no scene indices)", i, descs[i].scene_rows);
         } else if (descs[i].kind == IK_TERM_POSITION || descs[i].kind == IK_TERM_ROTATION || descs[i].kind == IK_TERM_FRAME) {
             if (descs[i].num_frames < 1) {
                 delete T;

@@ -1,6 +1,7 @@
 """The continuous-batching server (ik_server_*): results alone vs in the mix, admission, relaunch, errors."""
 
 import time
+from dataclasses import replace
 
 import numpy as np
 import pytest
@@ -108,28 +109,46 @@ def test_server_errors(gpu):
     srv.close()
 
 
-def test_server_refuses_terms_with_per_problem_references(gpu, panda_collision_spec):
-    """A request carries only seeds and pose targets: joint-reference, velocity, scene and base-reference terms
-    are refused when the type is registered."""
-    from robokit_b200.geom import BoxGeom, Scene
+def test_server_serves_shared_references_and_refuses_per_problem_ones(gpu, panda_collision_spec):
+    """A request carries only seeds and pose targets, so a served type may hold joint-reference, velocity,
+    base-reference and scene terms whose reference is one shared row (a rest pose, one scene); its results equal
+    the batch solve of the same problems.  A per-problem reference or scene index is refused at registration."""
+    from robokit_b200.geom import BoxGeom, Scene, SphereGeom
     from robokit_b200.opt import LMOptimizerConfig
     from robokit_b200.robo.robot import Robot
-    from robokit_b200.terms.dense import (ConfigurationTask, PositionTask, SceneCollisionTask, SmoothnessTask,
-                                          VelocityLimitTask)
+    from robokit_b200.terms.dense import ConfigurationTask, PositionTask, SceneCollisionTask, SmoothnessTask
 
     robot = Robot(panda_collision_spec)
     hand = robot.link_names.index("panda_hand")
-    pose = PositionTask(robot, hand, np.tile(np.array([0.4, 0, 0.4, 1, 0, 0, 0], np.float32), (1, 1, 1)))
-    prev = robot.state(panda_collision_spec.zero_q[None].astype(np.float32))
-    others = [SmoothnessTask(robot=robot, prev_var=prev, weight=1.0),
-              ConfigurationTask(robot=robot, rest_q=panda_collision_spec.zero_q.astype(np.float32), weight=1.0),
-              VelocityLimitTask(robot=robot, dt=0.1, prev_state_var=prev, weight=1.0),
-              SceneCollisionTask(robot, Scene(1).add(BoxGeom([[0.1, 0.1, 0.1]], [0, 1])), weight=1.0)]
+    n = 48
+    q0 = robot.sample_q(n, seed=3)
+    T = robot.forward_kinematics(robot.state(robot.sample_q(n, seed=4))).get_T_world_link(hand).numpy()
+    rest = panda_collision_spec.midrange_q.astype(np.float32)
+    scene = Scene(1).add(BoxGeom([[0.1, 0.1, 0.1]], [0, 1], poses=[[0.5, 0.0, 0.3, 1, 0, 0, 0]]))
+    lm = LMOptimizerConfig(max_iter=20, early_stopping_interval=0)
+
+    def extra():
+        return [ConfigurationTask(robot=robot, rest_q=rest, weight=0.1),
+                SceneCollisionTask(robot, scene, weight=5.0, margin=0.05)]
+
+    placeholder = PositionTask(robot, hand, T[:1].reshape(1, 1, 7), weight=10.0)
     srv = serve.IKServer(budget_bytes=64 << 20)
     try:
-        for t in others:
-            with pytest.raises(N.NativeError, match="not served"):
-                srv.add_type(robot, [pose, t], LMOptimizerConfig(max_iter=5, early_stopping_interval=0), 16)
-        assert srv.add_type(robot, [pose], LMOptimizerConfig(max_iter=5, early_stopping_interval=0), 16) == 0
+        tid = srv.add_type(robot, [placeholder, *extra()], lm, 64)
+        rid = srv.submit(tid, q0, [T.reshape(n, 1, 7)])
+        got = srv.wait([rid], timeout_s=60)[rid]
+        opt = LMOptimizer([PositionTask(robot, hand, T.reshape(n, 1, 7), weight=10.0), *extra()],
+                          replace(lm, form="persistent"))
+        state = robot.state(q0.copy())
+        opt.solve(VarValues({VarKey.ROBOT: state}))
+        np.testing.assert_allclose(got["q"], state.q.numpy(), rtol=0, atol=1e-4)
+        np.testing.assert_allclose(got["cost"], opt.costs.numpy(), rtol=1e-4, atol=1e-9)
+        prev4 = robot.state(np.zeros((4, robot.num_actuated_joints), np.float32))
+        with pytest.raises(N.NativeError, match="one shared reference row"):
+            srv.add_type(robot, [placeholder, SmoothnessTask(robot=robot, prev_var=prev4, weight=1.0)], lm, 16)
+        two = Scene(2).add(SphereGeom([0.1, 0.1], [0, 1, 2]))
+        with pytest.raises(ValueError, match="scene_indices"):  # per-problem scenes do not lower to one row
+            srv.add_type(robot, [placeholder, SceneCollisionTask(robot, two, scene_indices=N.DeviceArray.from_numpy(
+                np.array([0, 1], np.int32)), weight=1.0)], lm, 16)
     finally:
         srv.close()
