@@ -152,3 +152,43 @@ def test_server_serves_shared_references_and_refuses_per_problem_ones(gpu, panda
                 np.array([0, 1], np.int32)), weight=1.0)], lm, 16)
     finally:
         srv.close()
+
+
+def test_server_serves_velocity_and_base_references(gpu, panda_collision_spec):
+    """The remaining shared-reference kinds: a velocity limit against a fixed previous state, and the base rows
+    of a ConfigurationTask on a floating base; served results equal the batch solve."""
+    from robokit_b200.opt import LMOptimizerConfig
+    from robokit_b200.robo.robot import Robot
+    from robokit_b200.terms.dense import ConfigurationTask, PositionTask, VelocityLimitTask
+
+    robot = Robot(panda_collision_spec)
+    hand = robot.link_names.index("panda_hand")
+    n = 32
+    q0 = robot.sample_q(n, seed=8)
+    base0 = np.tile(np.array([0.05, -0.02, 0.0, 1, 0, 0, 0], np.float32), (n, 1))
+    T = robot.forward_kinematics(robot.state(robot.sample_q(n, seed=9))).get_T_world_link(hand).numpy()
+    T[:, 0] += 0.2
+    prev = robot.state(panda_collision_spec.midrange_q[None].astype(np.float32))
+    rest_base = np.array([[0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0]], np.float32)
+    lm = LMOptimizerConfig(max_iter=20, early_stopping_interval=0)
+
+    def extra():
+        return [VelocityLimitTask(robot=robot, dt=0.5, prev_state_var=prev, weight=1.0),
+                ConfigurationTask(robot=robot, rest_q=panda_collision_spec.zero_q.astype(np.float32),
+                                  T_world_base_rest=rest_base, weight=0.01, base_weight=[1, 1, 10, 10, 10, 1])]
+
+    srv = serve.IKServer(budget_bytes=64 << 20)
+    try:
+        tid = srv.add_type(robot, [PositionTask(robot, hand, T[:1].reshape(1, 1, 7), weight=10.0), *extra()], lm, 64,
+                           floating=True)
+        rid = srv.submit(tid, q0, [T.reshape(n, 1, 7)], base0)
+        got = srv.wait([rid], timeout_s=60)[rid]
+        opt = LMOptimizer([PositionTask(robot, hand, T.reshape(n, 1, 7), weight=10.0), *extra()],
+                          replace(lm, form="persistent"))
+        state = robot.state(q0.copy(), base0.copy())
+        opt.solve(VarValues({VarKey.ROBOT: state}))
+        np.testing.assert_allclose(got["q"], state.q.numpy(), rtol=0, atol=1e-4)
+        np.testing.assert_allclose(got["base"], state.T_world_base.numpy(), rtol=0, atol=1e-4)
+        np.testing.assert_allclose(got["cost"], opt.costs.numpy(), rtol=1e-4, atol=1e-9)
+    finally:
+        srv.close()
